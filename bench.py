@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Benchmark: the full frame-to-depth pipeline on one 728x544 pair with 128
+disparities and 8 paths (Rectification -> Disparity -> SpeckleFilter -> Depth
+-> PointCloud(decimation 4)), pairs/s.
+
+A step is one pair through the pipeline. `value` times the device pipeline on
+inputs already in HBM (per-step CUDA events on the launching stream, L2
+flushed between steps outside the events); `e2e` times the same pipeline
+through the public API (CudaSegment.send_request / await_) from host frames,
+host<->device copies included, up to depth() pairs in flight. Multi-GPU runs
+are independent replicas (pairs do not shard: SGM paths cross the whole
+image), timed as the max over ranks.
+
+`--impl reference` times the reference's CPU formulation of the same pipeline
+(the oracle's C port of the reference's Rust matcher and stages) on all host
+threads, one pair per thread per step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "pairs/s at 728x544x128 d, 8 paths (full frame-to-depth pipeline)"
+WIDTH, HEIGHT, DISPARITIES, PATHS = 728, 544, 128, 8
+DECIMATION = 4
+KERNELS_PER_STEP = 11  # rectify x2, census, costs, paths, select, check, median, despeckle, depth, cloud
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--inputs", type=int, default=8, help="distinct pairs cycled through")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        return float(m["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- inputs
+def make_inputs(count, seed):
+    from nx_stereo_b200 import scene
+
+    rig = scene.rig(WIDTH, HEIGHT)
+    frames = []
+    for i in range(count):
+        left, right = scene.rectified_pair(WIDTH, HEIGHT, seed=seed * 1000 + i, rectangles=6,
+                                           min_disparity=4, max_disparity=120)
+        frames.append(scene.raw_frames(left, right, rig))
+    return rig, frames
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_id):
+        self.samples = []
+        self.proc = None
+        self.device_id = device_id
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+               "-lms", "200"]
+        if self.device_id is not None:
+            cmd += ["-i", str(self.device_id)]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append((time.monotonic(), [f.strip() for f in line.split(",")]))
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self, t0, t1):
+        rows = [s for t, s in self.samples if t0 - 0.25 <= t <= t1 + 0.25] or \
+            [s for _, s in self.samples]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": num(rows[0][2]), "reasons": reasons, "samples": len(rows),
+                "power_w_max": max((num(r[3]) or 0.0) for r in rows)}
+
+
+# ---------------------------------------------------------------- our arm
+class DevicePipeline:
+    """The pipeline's kernels on device buffers, one C-ABI call per stage; CUDA
+    events bracket the path-aggregation kernel (the dominant one)."""
+
+    def __init__(self, native, torch, ctx, rig, stream):
+        from nx_stereo_b200 import scene
+
+        self.native, self.torch, self.ctx, self.stream = native, torch, ctx, stream
+        cams = scene.cameras(rig)
+        self.cameras = [native.make_camera(cams[s]["k"], cams[s]["d"], cams[s]["inverse_pr"])
+                        for s in ("left", "right")]
+        self.focal, self.baseline = rig["focal_length_px"], rig["baseline_m"]
+        self.cx, self.cy = rig["principal_point"]
+        px, vol = WIDTH * HEIGHT, WIDTH * HEIGHT * DISPARITIES
+        dev = torch.device("cuda")
+        u8, f32 = torch.uint8, torch.float32
+        self.images = torch.empty((2, HEIGHT, WIDTH), dtype=u8, device=dev)
+        self.codes = torch.empty((2, HEIGHT, WIDTH), dtype=torch.int64, device=dev)
+        self.costs = torch.empty(vol, dtype=u8, device=dev)
+        self.volumes = torch.empty(PATHS * vol, dtype=u8, device=dev)
+        self.selected = torch.empty(px, dtype=f32, device=dev)
+        self.keys = torch.empty(px, dtype=torch.int32, device=dev)
+        self.checked = torch.empty(px, dtype=f32, device=dev)
+        self.disparity = torch.empty(px, dtype=f32, device=dev)
+        self.speckled = torch.empty(px, dtype=f32, device=dev)
+        self.depth_mm = torch.empty(px, dtype=torch.int16, device=dev)
+        self.depth_m = torch.empty(px, dtype=f32, device=dev)
+        self.grid = torch.empty((HEIGHT // DECIMATION) * (WIDTH // DECIMATION) * 3, dtype=f32,
+                                device=dev)
+        self.kept = torch.empty(1, dtype=torch.int32, device=dev)
+
+    def step(self, frames, paths_events=None):
+        n, s, call = self.native, self.stream, self.native.call
+        import ctypes
+
+        for side in range(2):
+            call("nxs_rectify_device", frames[side].data_ptr(), WIDTH, HEIGHT,
+                 ctypes.byref(self.cameras[side]), WIDTH, HEIGHT,
+                 self.images[side].data_ptr(), s)
+        call("nxs_census_device", self.images[0].data_ptr(), WIDTH, HEIGHT,
+             self.codes[0].data_ptr(), s)
+        call("nxs_census_device", self.images[1].data_ptr(), WIDTH, HEIGHT,
+             self.codes[1].data_ptr(), s)
+        call("nxs_costs_device", self.codes[0].data_ptr(), self.codes[1].data_ptr(), WIDTH,
+             HEIGHT, DISPARITIES, self.costs.data_ptr(), s)
+        if paths_events:
+            paths_events[0].record()
+        call("nxs_paths_device", self.costs.data_ptr(), WIDTH, HEIGHT, DISPARITIES, PATHS, 8, 64,
+             self.volumes.data_ptr(), s)
+        if paths_events:
+            paths_events[1].record()
+        call("nxs_select_paths_device", self.volumes.data_ptr(), WIDTH, HEIGHT, DISPARITIES,
+             PATHS, 1.0526315789473684, self.selected.data_ptr(), self.keys.data_ptr(), s)
+        call("nxs_consistency_device", self.selected.data_ptr(), self.keys.data_ptr(), WIDTH,
+             HEIGHT, self.checked.data_ptr(), s)
+        call("nxs_median3_device", self.checked.data_ptr(), WIDTH, HEIGHT, 1,
+             self.disparity.data_ptr(), s)
+        call("nxs_despeckle_device", self.disparity.data_ptr(), WIDTH, HEIGHT, 12.0, 1.0, 3,
+             self.speckled.data_ptr(), s)
+        call("nxs_depth_device", self.speckled.data_ptr(), WIDTH * HEIGHT, self.focal,
+             self.baseline, self.depth_mm.data_ptr(), self.depth_m.data_ptr(), s)
+        call("nxs_cloud_device", self.depth_m.data_ptr(), WIDTH, HEIGHT, DECIMATION, self.focal,
+             self.cx, self.cy, 0.05, 20.0, self.grid.data_ptr(), self.kept.data_ptr(), s)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from nx_stereo_b200 import native, segment, stage
+
+    torch.cuda.set_device(local_rank)
+    native.load()
+    ctx = native.Context(local_rank)
+    rig, frames = make_inputs(args.inputs, seed=1 + rank)
+    stream_obj = torch.cuda.Stream()
+    dist = world > 1
+    if dist:
+        import torch.distributed as td
+
+    with torch.cuda.stream(stream_obj):
+        s = stream_obj.cuda_stream
+        pipe = DevicePipeline(native, torch, ctx, rig, s)
+        d_frames = [(torch.from_numpy(l).cuda(), torch.from_numpy(r).cuda()) for l, r in frames]
+        flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+        for i in range(args.warmup):
+            pipe.step(d_frames[i % len(d_frames)])
+        torch.cuda.synchronize()
+        if dist:
+            td.barrier()
+        sampler = ClockSampler(local_rank if os.environ.get("CUDA_VISIBLE_DEVICES") is None else None)
+        sampler.start()
+        time.sleep(0.3)
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        paths_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                    for _ in range(args.steps)]
+        torch.cuda.synchronize()
+        t0 = time.monotonic()
+        for i in range(args.steps):
+            flush.fill_(i & 0xFF)  # evict L2 between timed steps, outside the events
+            starts[i].record()
+            pipe.step(d_frames[i % len(d_frames)], paths_ev[i])
+            ends[i].record()
+        torch.cuda.synchronize()
+        t1 = time.monotonic()
+        step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+        paths_ms = [a.elapsed_time(b) for a, b in paths_ev]
+    total_s = sum(step_ms) / 1000.0
+    if dist:
+        t = torch.tensor([total_s], device="cuda", dtype=torch.float64)
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        total_s = float(t.item())
+    value = world * args.steps / total_s
+
+    # e2e: the public API, host frames in, outputs back to the host.
+    geometry = segment.standard_geometry(WIDTH, HEIGHT, the_rig=rig)
+    status, members = segment.members(
+        [stage.Rectification, (stage.Disparity, {"num_disparities": DISPARITIES}),
+         stage.SpeckleFilter, stage.Depth, (stage.PointCloud, {"decimation": DECIMATION})],
+        geometry)
+    assert status == "ok", members
+    status, seg = segment.CudaSegment.build(members, geometry, {"device": local_rank})
+    assert status == "ok", seg
+    mod = segment.CudaSegment
+    entries = [{"left_frame": l, "right_frame": r} for l, r in frames]
+    h2d = sum(a.nbytes for a in entries[0].values())
+    d2h = None
+
+    def e2e_loop(count):
+        nonlocal d2h
+        inflight = []
+        for i in range(count):
+            status, req = mod.send_request(entries[i % len(entries)], seg)
+            assert status == "ok", req
+            inflight.append(req)
+            if len(inflight) >= mod.depth():
+                reply = mod.await_(inflight.pop(0), seg, 60000)
+                assert reply[0] == "ok", reply
+                d2h = sum(v.nbytes for v in reply[1].values())
+        while inflight:
+            reply = mod.await_(inflight.pop(0), seg, 60000)
+            assert reply[0] == "ok", reply
+            d2h = sum(v.nbytes for v in reply[1].values())
+
+    e2e_loop(max(args.warmup, mod.depth()))
+    torch.cuda.synchronize()
+    if dist:
+        td.barrier()
+    e0 = time.perf_counter()
+    e2e_loop(args.steps)
+    torch.cuda.synchronize()
+    e_s = time.perf_counter() - e0
+    if dist:
+        t = torch.tensor([e_s], device="cuda", dtype=torch.float64)
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        e_s = float(t.item())
+    sampler.stop()
+    clocks = sampler.summary(t0, t1)
+    seg.release()
+
+    peak, peak_kind = peaks()
+    px, vol = WIDTH * HEIGHT, WIDTH * HEIGHT * DISPARITIES
+    paths_bytes = vol + PATHS * vol  # u8 costs read once, 8 u8 path volumes written
+    paths_avg_s = statistics.mean(paths_ms) / 1000.0
+    achieved = paths_bytes / paths_avg_s / 1e9
+    b_alg = 8 * vol + 6 * px  # per pair: u16 cost + aggregate written and read, images, disparity
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(statistics.mean(step_ms), 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/u16",
+        "data": "synthetic (seeded piecewise-planar scenes, raw frames from a synthetic rig)",
+        "config": {"workload": "full pipeline 728x544 frames -> 728x544, D128, 8 paths, "
+                               "despeckle, depth, cloud (decimation 4)",
+                   "width": WIDTH, "height": HEIGHT, "disparities": DISPARITIES, "paths": PATHS,
+                   "pairs_per_step": 1, "parallelism": f"replicas x{world}",
+                   "l2": "flushed between steps (256 MiB write outside the step events); "
+                         "per-step working set 460 MB > 126 MB L2"},
+        "mdisp_s": round(value * px * DISPARITIES / 1e6, 1),
+        "gpu_launches": KERNELS_PER_STEP * args.steps,
+        "roofline": {"bound": "hbm", "kernel": "paths_kernel (8-path aggregation)",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": paths_bytes,
+                     "avg_launch_ms": round(paths_avg_s * 1000, 4), "traffic": None},
+        "pipeline_roofline": {"b_alg_per_pair": b_alg,
+                              "achieved_gbs": round(b_alg * value / world / 1e9, 1),
+                              "frac": round(b_alg * value / world / 1e9 / peak, 4)},
+        "e2e": {"value": round(world * args.steps / e_s, 2), "unit": "pairs/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "api": "CudaSegment.send_request/await_ (C ABI nxs_run_async), depth "
+                       f"{mod.depth()}"},
+        "clocks": clocks,
+    }
+    return line
+
+
+def cpu_sample(rig, frames, threads, pairs):
+    from nx_stereo_b200 import scene
+    from oracle import oracle
+
+    cams = scene.cameras(rig)
+    cl = oracle.make_camera(cams["left"]["k"], cams["left"]["d"], cams["left"]["inverse_pr"])
+    cr = oracle.make_camera(cams["right"]["k"], cams["right"]["d"], cams["right"]["inverse_pr"])
+    lefts = np.stack([frames[i % len(frames)][0] for i in range(pairs)])
+    rights = np.stack([frames[i % len(frames)][1] for i in range(pairs)])
+    t = time.perf_counter()
+    oracle.fast_pipeline_batch(lefts, rights, cl, cr, (HEIGHT, WIDTH), DISPARITIES, PATHS,
+                               focal_length_px=rig["focal_length_px"],
+                               baseline_m=rig["baseline_m"], decimation=DECIMATION,
+                               principal_point=rig["principal_point"], threads=threads)
+    return pairs / (time.perf_counter() - t)
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    threads = host_threads()
+    rig, frames = make_inputs(min(args.inputs, 4), seed=1)
+    values = []
+    for i in range(args.warmup + args.steps):
+        v = cpu_sample(rig, frames, threads, threads)
+        if i >= args.warmup:
+            values.append(v)
+    value = statistics.mean(values)
+    sample = f"{threads} pairs per step (one per thread), {args.steps} steps"
+    return {"metric": METRIC, "value": round(value, 3), "unit": "pairs/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * threads / value, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/u16",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": "full pipeline 728x544 frames -> 728x544, D128, 8 paths, "
+                                   "despeckle, depth, cloud (decimation 4)"},
+            "cpu_baseline": {"value": round(value, 3), "unit": "pairs/s", "cores": threads,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": round(value, 3), "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference(args)))
+        return 0
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as td
+
+        torch.cuda.set_device(local_rank)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                              device_id=torch.device("cuda", local_rank))
+    line = run_ours(args, rank, world, local_rank)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = host_threads()
+        rig, frames = make_inputs(4, seed=1)
+        value = cpu_sample(rig, frames, threads, threads)
+        line["cpu_baseline"] = {"value": round(value, 3), "unit": "pairs/s", "cores": threads,
+                                "kind": "port",
+                                "sample": f"{threads} pairs, one per host thread (C port of the "
+                                          "reference's Rust pipeline)"}
+    if world > 1:
+        import torch.distributed as td
+
+        td.barrier()
+        td.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,299 @@
+/*
+ * nx_stereo_b200: NxStereo's full-search Stage.Disparity path (census, Hamming
+ * costs, 8- or 3-path SGM, winner-take-all with uniqueness, subpixel, the
+ * left-right check and the median) with Stage.Rectification,
+ * Stage.SpeckleFilter and the stages after them, as CUDA kernels for B200
+ * (sm_100a) behind a C ABI.
+ *
+ * Two layers:
+ *
+ *  1. The segment protocol: configure / run / release, the three requests the
+ *     reference's native Port serves (native/stereo_match/src/protocol.rs:1-23),
+ *     as in-process calls an Erlang NIF (or ctypes, cgo, JNI) binds. A segment is
+ *     a run of stages configured once, fed one pair per request, FIFO, with the
+ *     values its stages carry from pair to pair kept on the device.
+ *
+ *  2. Direct entry points: the matcher on one pair (NxStereo.sgm/3) and each
+ *     stage kernel on device buffers, for callers that manage their own memory
+ *     and streams, and for checking intermediates bit for bit.
+ *
+ * Conventions: images are row-major, width fastest. Every call returns an
+ * nxs_status; on failure a UTF-8 message is written to `error` (at most
+ * error_len bytes including the terminating zero) when `error` is not NULL.
+ * No exception crosses the ABI. Pointers named `d_*` are device pointers;
+ * `stream` is a cudaStream_t (NULL for the legacy default stream).
+ */
+#ifndef NX_STEREO_B200_H
+#define NX_STEREO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    NXS_OK = 0,
+    NXS_PENDING = 1,       /* a request is still on the device */
+    NXS_REFUSED = 2,       /* a configuration the segment refuses: {:stop, reason} */
+    NXS_BAD_RUN = 3,       /* a request the segment cannot run: {:error, reason} */
+    NXS_CUDA_ERROR = 4,    /* the device failed */
+    NXS_TIMEOUT = 5,       /* a wait ran out */
+    NXS_BAD_ARGUMENT = 6,  /* a direct entry point's arguments are out of range */
+    NXS_NO_SEGMENT = 7     /* no segment of that id is configured */
+} nxs_status;
+
+/* Element types: the Port's tensor type codes (native/stereo_match/src/tensor.rs:25-30). */
+enum { NXS_U8 = 0, NXS_U16 = 1, NXS_F32 = 2, NXS_S32 = 3 };
+
+typedef struct nxs_context nxs_context;
+typedef struct nxs_request nxs_request;
+
+/* ------------------------------------------------------------------------ */
+/* Context                                                                   */
+
+/* Opens a context on CUDA device `device`. Replaces starting the Port
+ * (lib/nx_stereo/matcher.ex:248-260, native/stereo_match/src/main.rs:21-38). */
+nxs_status nxs_create(int device, nxs_context **context, char *error, size_t error_len);
+
+/* Releases every segment and the context's device memory. */
+void nxs_destroy(nxs_context *context);
+
+/* The library's version string. */
+const char *nxs_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Layer 1: the segment protocol                                             */
+
+/* A stage's build setting or native constant, as the configure request
+ * carries them: a name and an f64 (lib/nx_stereo/native_segment.ex:256-290). */
+typedef struct {
+    const char *name;
+    double value;
+} nxs_setting;
+
+/* A member: its native kind ("rectification", "disparity", "speckle_filter",
+ * "temporal_filter", "depth", "point_cloud", "quality") and its settings. */
+typedef struct {
+    const char *kind;
+    uint32_t n_settings;
+    const nxs_setting *settings;
+} nxs_member;
+
+/* The sizes every stage works with (native/stereo_match/src/segment.rs:19-27). */
+typedef struct {
+    uint32_t width, height;             /* the rectified working size */
+    uint32_t frame_width, frame_height; /* the camera frames' size */
+} nxs_geometry;
+
+/* A live input of a member for one pair: a name and its f32 values, as the
+ * run request flattens a stage's params/2 (native_segment.ex:292-322;
+ * e.g. "p1", "uniqueness", "left.k", "right.inverse_pr"). */
+typedef struct {
+    const char *name;
+    uint32_t count;
+    const float *values;
+} nxs_param;
+
+typedef struct {
+    uint32_t n_params;
+    const nxs_param *params;
+} nxs_member_params;
+
+/* A tensor entering a request (host memory, borrowed for the call only) or
+ * returned by one (owned by the request until nxs_request_free). */
+typedef struct {
+    const char *name;
+    uint32_t type; /* NXS_U8, NXS_U16, NXS_F32 or NXS_S32 */
+    uint32_t rank; /* 0 to 4 */
+    uint32_t dims[4];
+    const void *data;
+    uint64_t bytes;
+} nxs_tensor;
+
+/* Configures segment `segment` with `members` for `geometry`, replacing any
+ * segment of that id (which starts the values its stages carry over).
+ * NXS_REFUSED with the reason for a kind without an implementation, a
+ * setting a kind does not take, or frames smaller than the working size to
+ * rectify (native/stereo_match/src/segment.rs:181-333). Replaces the configure
+ * request (protocol.rs:5-9). */
+nxs_status nxs_configure(nxs_context *context, uint32_t segment, const nxs_geometry *geometry,
+                         uint32_t n_members, const nxs_member *members, char *error,
+                         size_t error_len);
+
+/* Called on a CUDA host-callback thread once a request's outputs are in host
+ * memory; it must not call CUDA. A NIF passes enif_send here. */
+typedef void (*nxs_done_fn)(void *user, uint64_t tag);
+
+/* Sends one pair through segment `segment` without waiting: copies the
+ * entries' host bytes into the request before returning, enqueues every
+ * stage on the segment's stream, and returns the request. Requests on one
+ * segment run in the order sent. NXS_BAD_RUN for missing, misshapen or
+ * mistyped entries or params; NXS_NO_SEGMENT for an unknown id. Replaces the
+ * run request (protocol.rs:10-15) and NativeSegment.send_request/2
+ * (lib/nx_stereo/native_segment.ex:164-189). */
+nxs_status nxs_run_async(nxs_context *context, uint32_t segment, uint32_t n_members,
+                         const nxs_member_params *params, uint32_t n_entries,
+                         const nxs_tensor *entries, nxs_done_fn done, void *user, uint64_t tag,
+                         nxs_request **request, char *error, size_t error_len);
+
+/* NXS_OK once the request is done, NXS_PENDING while it is on the device, or
+ * the device's error. */
+nxs_status nxs_request_poll(nxs_request *request, char *error, size_t error_len);
+
+/* Waits up to timeout_ms (negative: without limit) for the request: NXS_OK,
+ * NXS_TIMEOUT, or the device's error. Replaces NativeSegment.await/3
+ * (native_segment.ex:207-218). */
+nxs_status nxs_request_wait(nxs_request *request, int64_t timeout_ms, char *error,
+                            size_t error_len);
+
+/* The tensors the members filled, each once, in the order first filled
+ * (segment.rs:203-239); valid until nxs_request_free. */
+nxs_status nxs_request_outputs(nxs_request *request, uint32_t *n_outputs,
+                               const nxs_tensor **outputs);
+
+/* Each member's device time in microseconds (the reply's times, protocol.rs:11-15). */
+nxs_status nxs_request_times(nxs_request *request, uint32_t *n_members,
+                             const uint32_t **times_us);
+
+/* Frees a request; waits for it first if it is still on the device. */
+void nxs_request_free(nxs_request *request);
+
+/* Releases segment `segment` after its requests finish. Replaces the release
+ * request (protocol.rs:16). */
+nxs_status nxs_release(nxs_context *context, uint32_t segment);
+
+/* ------------------------------------------------------------------------ */
+/* Layer 2: direct entry points                                              */
+
+/* NxStereo.sgm/3's settings (lib/nx_stereo.ex:44-62). disparities: 64 or 128
+ * as the reference takes them, and 96, 192 and 256 beyond it; paths 3 or 8;
+ * integers 0 <= p1 < p2 <= 79; uniqueness >= 1. */
+typedef struct {
+    uint32_t disparities;
+    uint32_t paths;
+    uint32_t p1, p2;
+    float uniqueness;
+    uint32_t stage_mask; /* non-zero: Stage.Disparity's step, disparity <= 0 becomes -1 */
+} nxs_sgm_params;
+
+/* Why NxStereo.sgm/3 would refuse these settings for a width x height pair
+ * (lib/nx_stereo.ex:89-134, native/stereo_match/src/lib.rs:41-72), extended to
+ * the disparity counts above: NXS_OK or NXS_BAD_ARGUMENT with the reason. */
+nxs_status nxs_sgm_check(const nxs_sgm_params *params, uint32_t width, uint32_t height,
+                         char *error, size_t error_len);
+
+/* The disparity of each left pixel, -1.0 where unmatched: NxStereo.sgm/3 on a
+ * rectified u8 pair in host memory (lib/nx_stereo.ex:64-74; natively
+ * Matcher::disparity, native/stereo_match/src/lib.rs:105-124). Synchronous. */
+nxs_status nxs_sgm(nxs_context *context, const uint8_t *left, const uint8_t *right,
+                   uint32_t width, uint32_t height, const nxs_sgm_params *params,
+                   float *disparity, char *error, size_t error_len);
+
+/* The same on device buffers, enqueued on `stream` (the context's scratch is
+ * used: one call at a time per context and stream). */
+nxs_status nxs_sgm_device(nxs_context *context, const uint8_t *d_left, const uint8_t *d_right,
+                          uint32_t width, uint32_t height, const nxs_sgm_params *params,
+                          float *d_disparity, void *stream, char *error, size_t error_len);
+
+/* The matcher's device scratch, in bytes, for one pair of this size. */
+uint64_t nxs_sgm_scratch_bytes(uint32_t width, uint32_t height, uint32_t disparities);
+
+/* --- the matcher's steps, for checking intermediates (device buffers) --- */
+
+/* 48-bit 9x7 census codes, u64 per pixel (lib/nx_stereo.ex:491-505). */
+nxs_status nxs_census_device(const uint8_t *d_image, uint32_t width, uint32_t height,
+                             uint64_t *d_codes, void *stream);
+
+/* u8 Hamming costs, [height][width][disparities] (lib/nx_stereo.ex:528-542). */
+nxs_status nxs_costs_device(const uint64_t *d_left_codes, const uint64_t *d_right_codes,
+                            uint32_t width, uint32_t height, uint32_t disparities,
+                            uint8_t *d_costs, void *stream);
+
+/* The sum of the path costs over every direction, u16
+ * [height][width][disparities] (lib/nx_stereo.ex:544-606). Uses the context's
+ * scratch. */
+nxs_status nxs_aggregate_device(nxs_context *context, const uint8_t *d_costs, uint32_t width,
+                                uint32_t height, uint32_t disparities, uint32_t paths,
+                                uint32_t p1, uint32_t p2, uint16_t *d_sums, void *stream);
+
+/* Each direction's path costs, u8 [paths][height][width][disparities], the
+ * directions in the reference's order (lib/nx_stereo.ex:544-606): one warp per
+ * scan line. d_paths holds `paths` volumes. */
+nxs_status nxs_paths_device(const uint8_t *d_costs, uint32_t width, uint32_t height,
+                            uint32_t disparities, uint32_t paths, uint32_t p1, uint32_t p2,
+                            uint8_t *d_paths, void *stream);
+
+/* Selection straight from the path volumes: their sum, winner, uniqueness and
+ * subpixel (lib/nx_stereo.ex:608-641). */
+nxs_status nxs_select_paths_device(const uint8_t *d_paths, uint32_t width, uint32_t height,
+                                   uint32_t disparities, uint32_t paths, float uniqueness,
+                                   float *d_disparity, uint32_t *d_keys, void *stream);
+
+/* Winner, uniqueness and subpixel from u16 sums: f32 disparity and u32 keys
+ * (lib/nx_stereo.ex:608-641). */
+nxs_status nxs_select_device(const uint16_t *d_sums, uint32_t width, uint32_t height,
+                             uint32_t disparities, float uniqueness, float *d_disparity,
+                             uint32_t *d_keys, void *stream);
+
+/* The left-right check (lib/nx_stereo.ex:643-683). */
+nxs_status nxs_consistency_device(const float *d_disparity, const uint32_t *d_keys,
+                                  uint32_t width, uint32_t height, float *d_checked,
+                                  void *stream);
+
+/* The 3x3 median (lib/nx_stereo/image.ex:483-505), then, when stage_mask is
+ * non-zero, Stage.Disparity's mask (stage/disparity.ex:162). */
+nxs_status nxs_median3_device(const float *d_image, uint32_t width, uint32_t height,
+                              uint32_t stage_mask, float *d_filtered, void *stream);
+
+/* --- the stages around the matcher (device buffers) --- */
+
+/* A camera as NxStereo.Rectify.camera/4 builds it, rows moved by the stage
+ * (lib/nx_stereo/rectify.ex:20-50, stage/rectification.ex:84-89): the camera
+ * matrix, the plumb_bob coefficients k1 k2 p1 p2 k3 and the inverse of
+ * (rectified camera matrix x rectifying rotation), row-major f32. */
+typedef struct {
+    float k[9];
+    float d[5];
+    float inverse_pr[9];
+} nxs_camera;
+
+/* NxStereo.Rectify.rectify/3 of a frame to width x height
+ * (lib/nx_stereo/rectify.ex:133-207). Frames must be at least the working
+ * size (stage/rectification.ex:75-82). */
+nxs_status nxs_rectify_device(const uint8_t *d_frame, uint32_t frame_width,
+                              uint32_t frame_height, const nxs_camera *camera, uint32_t width,
+                              uint32_t height, uint8_t *d_rectified, void *stream);
+
+/* NxStereo.Filter.despeckle/2 (lib/nx_stereo/filter.ex:14-80); radius 1..8. */
+nxs_status nxs_despeckle_device(const float *d_disparity, uint32_t width, uint32_t height,
+                                float min_support, float max_diff, uint32_t radius,
+                                float *d_despeckled, void *stream);
+
+/* NxStereo.Filter.temporal/4 in place (lib/nx_stereo/filter.ex:82-130). */
+nxs_status nxs_temporal_device(float *d_disparity, float *d_previous, float *d_missed,
+                               uint64_t pixels, float alpha, float delta, float hold,
+                               float max_missed, void *stream);
+
+/* NxStereo.Depth.depth/3 (lib/nx_stereo/depth.ex:8-32). */
+nxs_status nxs_depth_device(const float *d_disparity, uint64_t pixels, float focal_length_px,
+                            float baseline_m, uint16_t *d_depth_mm, float *d_depth_m,
+                            void *stream);
+
+/* NxStereo.Depth.point_cloud/5 (lib/nx_stereo/depth.ex:34-89): the
+ * {height/decimation, width/decimation, 3} grid and the kept count (s32). */
+nxs_status nxs_cloud_device(const float *d_depth_m, uint32_t width, uint32_t height,
+                            uint32_t decimation, float focal_length_px, float cx, float cy,
+                            float nearest_m, float farthest_m, float *d_grid, int32_t *d_kept,
+                            void *stream);
+
+/* Stage.Quality's sums (lib/nx_stereo/diagnostics.ex:258-271), f32[5]; then
+ * previous := disparity. */
+nxs_status nxs_quality_device(const float *d_disparity, float *d_previous, uint32_t width,
+                              uint32_t height, float *d_sums, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

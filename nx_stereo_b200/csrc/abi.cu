@@ -1,0 +1,1163 @@
+// The C ABI of include/nx_stereo_b200.h: contexts, the segment protocol
+// (configure / run / release, the reference Port's three requests) and the
+// direct entry points.
+//
+// A segment owns a CUDA stream, its device buffers and what its stages carry
+// from pair to pair (the temporal filter's previous disparity and missed
+// counts, the quality stage's previous disparity). A request copies its
+// entries into pinned memory, enqueues the host-to-device copies, every
+// member's kernels and the device-to-host copies of the outputs on the
+// segment's stream, and returns; requests on one segment therefore run in
+// the order sent, as the reference's Port computes them
+// (native/stereo_match/src/main.rs:1-11).
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/nx_stereo_b200.h"
+#include "nxs_kernels.h"
+
+using namespace nxs;
+
+namespace {
+
+void set_error(char *error, size_t error_len, const char *format, ...) {
+    if (!error || error_len == 0) return;
+    va_list args;
+    va_start(args, format);
+    vsnprintf(error, error_len, format, args);
+    va_end(args);
+}
+
+nxs_status cuda_status(cudaError_t e, char *error, size_t error_len, const char *what) {
+    if (e == cudaSuccess) return NXS_OK;
+    set_error(error, error_len, "%s: %s", what, cudaGetErrorString(e));
+    return NXS_CUDA_ERROR;
+}
+
+// A device allocation that grows on demand.
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t n) {
+        if (n <= bytes) return cudaSuccess;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&ptr, n);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+// Pinned host blocks recycled between requests of one segment.
+struct PinnedPool {
+    std::mutex lock;
+    std::multimap<size_t, void *> free_blocks;
+    void *take(size_t n) {
+        {
+            std::lock_guard<std::mutex> g(lock);
+            auto it = free_blocks.lower_bound(n);
+            if (it != free_blocks.end() && it->first <= 4 * n + 4096) {
+                void *p = it->second;
+                free_blocks.erase(it);
+                return p;
+            }
+        }
+        void *p = nullptr;
+        if (cudaHostAlloc(&p, std::max<size_t>(n, 64), cudaHostAllocDefault) != cudaSuccess)
+            return nullptr;
+        std::lock_guard<std::mutex> g(lock);
+        sizes[p] = std::max<size_t>(n, 64);
+        return p;
+    }
+    void give(void *p) {
+        if (!p) return;
+        std::lock_guard<std::mutex> g(lock);
+        free_blocks.emplace(sizes[p], p);
+    }
+    ~PinnedPool() {
+        for (auto &kv : sizes) cudaFreeHost(kv.first);
+    }
+    std::map<void *, size_t> sizes;
+};
+
+enum class Kind { Rectification, Disparity, Speckle, Temporal, Depth, Cloud, Quality };
+
+struct Member {
+    Kind kind;
+    std::string kind_name;
+    int disparities = 0, paths = 0, radius = 3, decimation = 1;
+    float max_missed = 255.0f, min_depth_m = 0.0f, max_depth_m = INFINITY;
+    // carried from pair to pair
+    float *previous = nullptr, *missed = nullptr;
+};
+
+struct Spec {
+    std::string name;
+    uint32_t type;
+    std::vector<uint32_t> dims;
+    size_t bytes() const {
+        size_t n = type == NXS_U8 ? 1 : (type == NXS_U16 ? 2 : 4);
+        for (uint32_t d : dims) n *= d;
+        return n;
+    }
+};
+
+struct Segment {
+    uint32_t id = 0;
+    int device = 0;
+    nxs_geometry g{};
+    std::vector<Member> members;
+    std::vector<Spec> entries, outputs;
+    cudaStream_t stream = nullptr;
+    std::mutex order;  // one request enqueued at a time
+    PinnedPool pinned;
+    // device buffers
+    uint8_t *frames[2] = {nullptr, nullptr}, *images[2] = {nullptr, nullptr};
+    float *disparity[2] = {nullptr, nullptr}, *depth_m = nullptr, *grid = nullptr;
+    float *quality_sums = nullptr, *quality_columns = nullptr;
+    uint16_t *depth_mm = nullptr;
+    int32_t *kept = nullptr;
+    DeviceBuffer scratch;
+    std::vector<void *> allocations;
+
+    template <typename T>
+    cudaError_t alloc(T **p, size_t count) {
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+        if (e == cudaSuccess) {
+            allocations.push_back(q);
+            *p = static_cast<T *>(q);
+        }
+        return e;
+    }
+    ~Segment() {
+        cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        for (void *p : allocations) cudaFree(p);
+        scratch.release();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+}  // namespace
+
+struct nxs_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex lock;
+    std::map<uint32_t, std::shared_ptr<Segment>> segments;
+    DeviceBuffer scratch, io;
+};
+
+struct nxs_request {
+    std::shared_ptr<Segment> segment;
+    std::vector<void *> pinned;  // returned to the segment's pool on free
+    std::vector<cudaEvent_t> marks;  // before member 0, after each member
+    cudaEvent_t done = nullptr;
+    std::vector<nxs_tensor> outputs;
+    std::vector<std::string> names;
+    std::vector<uint32_t> times_us;
+    bool timed = false;
+    nxs_done_fn callback = nullptr;
+    void *user = nullptr;
+    uint64_t tag = 0;
+};
+
+// ---------------------------------------------------------------------------
+// Context
+
+extern "C" const char *nxs_version(void) { return "nx_stereo_b200 0.1 (sm_100a)"; }
+
+extern "C" nxs_status nxs_create(int device, nxs_context **context, char *error,
+                                 size_t error_len) {
+    if (!context) {
+        set_error(error, error_len, "context is NULL");
+        return NXS_BAD_ARGUMENT;
+    }
+    *context = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || device < 0 || device >= count) {
+        set_error(error, error_len, "no CUDA device %d (%d present%s%s)", device, count,
+                  e ? ": " : "", e ? cudaGetErrorString(e) : "");
+        return NXS_CUDA_ERROR;
+    }
+    if ((e = cudaSetDevice(device))) return cuda_status(e, error, error_len, "cudaSetDevice");
+    auto *c = new nxs_context();
+    c->device = device;
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking))) {
+        delete c;
+        return cuda_status(e, error, error_len, "cudaStreamCreate");
+    }
+    *context = c;
+    return NXS_OK;
+}
+
+extern "C" void nxs_destroy(nxs_context *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    {
+        std::lock_guard<std::mutex> g(c->lock);
+        c->segments.clear();
+    }
+    cudaStreamSynchronize(c->stream);
+    c->scratch.release();
+    c->io.release();
+    cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+// ---------------------------------------------------------------------------
+// Direct entry points
+
+static bool supported_disparities(uint32_t d) {
+    return d == 64 || d == 96 || d == 128 || d == 192 || d == 256;
+}
+
+extern "C" nxs_status nxs_sgm_check(const nxs_sgm_params *p, uint32_t width, uint32_t height,
+                                    char *error, size_t error_len) {
+    if (!p) {
+        set_error(error, error_len, "params is NULL");
+        return NXS_BAD_ARGUMENT;
+    }
+    // native/stereo_match/src/lib.rs:41-72 and lib/nx_stereo.ex:89-134.
+    if (!(width > 8 && height > 6 && width <= 4096)) {
+        set_error(error, error_len,
+                  "expected an image wider than 8, higher than 6 and at most 4096 wide, got %ux%u",
+                  width, height);
+        return NXS_BAD_ARGUMENT;
+    }
+    if (!supported_disparities(p->disparities)) {
+        set_error(error, error_len, "disparities must be 64, 96, 128, 192 or 256, got %u",
+                  p->disparities);
+        return NXS_BAD_ARGUMENT;
+    }
+    if (p->paths != 3 && p->paths != 8) {
+        set_error(error, error_len, "paths must be 3 or 8, got %u", p->paths);
+        return NXS_BAD_ARGUMENT;
+    }
+    if (!(p->p1 < p->p2 && p->p2 + 48 <= 127)) {
+        set_error(error, error_len, "expected 0 <= p1 < p2 <= 79, got %u and %u", p->p1, p->p2);
+        return NXS_BAD_ARGUMENT;
+    }
+    if (std::isnan(p->uniqueness) || p->uniqueness < 1.0f) {
+        set_error(error, error_len, "uniqueness must be at least 1.0, got %g",
+                  (double)p->uniqueness);
+        return NXS_BAD_ARGUMENT;
+    }
+    return NXS_OK;
+}
+
+extern "C" uint64_t nxs_sgm_scratch_bytes(uint32_t width, uint32_t height, uint32_t disparities) {
+    return matcher_scratch_bytes((int)width, (int)height, (int)disparities);
+}
+
+extern "C" nxs_status nxs_sgm_device(nxs_context *c, const uint8_t *d_left,
+                                     const uint8_t *d_right, uint32_t width, uint32_t height,
+                                     const nxs_sgm_params *p, float *d_disparity, void *stream,
+                                     char *error, size_t error_len) {
+    if (!c || !d_left || !d_right || !d_disparity) {
+        set_error(error, error_len, "a NULL context or buffer");
+        return NXS_BAD_ARGUMENT;
+    }
+    nxs_status s = nxs_sgm_check(p, width, height, error, error_len);
+    if (s) return s;
+    cudaSetDevice(c->device);
+    std::lock_guard<std::mutex> g(c->lock);
+    cudaError_t e = c->scratch.reserve(matcher_scratch_bytes(width, height, p->disparities));
+    if (e) return cuda_status(e, error, error_len, "scratch allocation");
+    MatcherScratch ms = carve_matcher_scratch(c->scratch.ptr, width, height, p->disparities);
+    e = run_matcher(d_left, d_right, width, height, p->disparities, p->paths, p->p1, p->p2,
+                    p->uniqueness, p->stage_mask ? 1 : 0, ms, d_disparity,
+                    static_cast<cudaStream_t>(stream));
+    return cuda_status(e, error, error_len, "matcher launch");
+}
+
+extern "C" nxs_status nxs_sgm(nxs_context *c, const uint8_t *left, const uint8_t *right,
+                              uint32_t width, uint32_t height, const nxs_sgm_params *p,
+                              float *disparity, char *error, size_t error_len) {
+    if (!c || !left || !right || !disparity) {
+        set_error(error, error_len, "a NULL context or buffer");
+        return NXS_BAD_ARGUMENT;
+    }
+    nxs_status s = nxs_sgm_check(p, width, height, error, error_len);
+    if (s) return s;
+    cudaSetDevice(c->device);
+    const size_t pixels = (size_t)width * height;
+    uint8_t *d_left, *d_right;
+    float *d_out;
+    {
+        std::lock_guard<std::mutex> g(c->lock);
+        cudaError_t e = c->io.reserve(2 * ((pixels + 255) & ~(size_t)255) + 4 * pixels);
+        if (e) return cuda_status(e, error, error_len, "buffer allocation");
+        d_left = static_cast<uint8_t *>(c->io.ptr);
+        d_right = d_left + ((pixels + 255) & ~(size_t)255);
+        d_out = reinterpret_cast<float *>(d_right + ((pixels + 255) & ~(size_t)255));
+    }
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(d_left, left, pixels, cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaMemcpyAsync(d_right, right, pixels, cudaMemcpyHostToDevice, c->stream)))
+        return cuda_status(e, error, error_len, "copy to the device");
+    s = nxs_sgm_device(c, d_left, d_right, width, height, p, d_out, c->stream, error, error_len);
+    if (s) return s;
+    if ((e = cudaMemcpyAsync(disparity, d_out, 4 * pixels, cudaMemcpyDeviceToHost, c->stream)) ||
+        (e = cudaStreamSynchronize(c->stream)))
+        return cuda_status(e, error, error_len, "matcher");
+    return NXS_OK;
+}
+
+#define CHECK_SIZE(cond)                   \
+    do {                                   \
+        if (!(cond)) return NXS_BAD_ARGUMENT; \
+    } while (0)
+
+extern "C" nxs_status nxs_census_device(const uint8_t *d_image, uint32_t width, uint32_t height,
+                                        uint64_t *d_codes, void *stream) {
+    CHECK_SIZE(d_image && d_codes && width > 0 && height > 0);
+    return launch_census(d_image, nullptr, width, height, d_codes, nullptr,
+                         static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_costs_device(const uint64_t *d_left_codes,
+                                       const uint64_t *d_right_codes, uint32_t width,
+                                       uint32_t height, uint32_t disparities, uint8_t *d_costs,
+                                       void *stream) {
+    CHECK_SIZE(d_left_codes && d_right_codes && d_costs && width > 0 && height > 0 &&
+               disparities % 16 == 0 && disparities >= 16 && disparities <= 256);
+    return launch_costs(d_left_codes, d_right_codes, width, height, disparities, d_costs,
+                        static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_aggregate_device(nxs_context *c, const uint8_t *d_costs,
+                                           uint32_t width, uint32_t height, uint32_t disparities,
+                                           uint32_t paths, uint32_t p1, uint32_t p2,
+                                           uint16_t *d_sums, void *stream) {
+    CHECK_SIZE(c && d_costs && d_sums && width > 0 && height > 0 && disparities % 16 == 0 &&
+               disparities >= 16 && disparities <= 256 && (paths == 3 || paths == 8) &&
+               p1 < p2 && p2 + 48 <= 127);
+    cudaSetDevice(c->device);
+    std::lock_guard<std::mutex> g(c->lock);
+    const size_t volume = (size_t)width * height * disparities;
+    if (c->scratch.reserve(8 * volume)) return NXS_CUDA_ERROR;
+    uint8_t *volumes = static_cast<uint8_t *>(c->scratch.ptr);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (launch_paths(d_costs, width, height, disparities, paths, p1, p2, volumes, s) ||
+        launch_sum_paths(volumes, width, height, disparities, paths, d_sums, s))
+        return NXS_CUDA_ERROR;
+    return NXS_OK;
+}
+
+extern "C" nxs_status nxs_paths_device(const uint8_t *d_costs, uint32_t width, uint32_t height,
+                                       uint32_t disparities, uint32_t paths, uint32_t p1,
+                                       uint32_t p2, uint8_t *d_paths, void *stream) {
+    CHECK_SIZE(d_costs && d_paths && width > 0 && height > 0 && disparities % 16 == 0 &&
+               disparities >= 16 && disparities <= 256 && (paths == 3 || paths == 8) &&
+               p1 < p2 && p2 + 48 <= 127);
+    return launch_paths(d_costs, width, height, disparities, paths, p1, p2, d_paths,
+                        static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_select_paths_device(const uint8_t *d_paths, uint32_t width,
+                                              uint32_t height, uint32_t disparities,
+                                              uint32_t paths, float uniqueness,
+                                              float *d_disparity, uint32_t *d_keys,
+                                              void *stream) {
+    CHECK_SIZE(d_paths && d_disparity && d_keys && width > 0 && height > 0 &&
+               disparities % 16 == 0 && disparities >= 16 && disparities <= 256 &&
+               (paths == 3 || paths == 8));
+    return launch_select_paths(d_paths, width, height, disparities, paths, uniqueness,
+                               d_disparity, d_keys, static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_select_device(const uint16_t *d_sums, uint32_t width, uint32_t height,
+                                        uint32_t disparities, float uniqueness,
+                                        float *d_disparity, uint32_t *d_keys, void *stream) {
+    CHECK_SIZE(d_sums && d_disparity && d_keys && width > 0 && height > 0 && disparities >= 4 &&
+               disparities <= 256 && disparities % 8 == 0);
+    return launch_select_sums(d_sums, width, height, disparities, uniqueness, d_disparity, d_keys,
+                              static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_consistency_device(const float *d_disparity, const uint32_t *d_keys,
+                                             uint32_t width, uint32_t height, float *d_checked,
+                                             void *stream) {
+    CHECK_SIZE(d_disparity && d_keys && d_checked && width > 0 && width <= 8192 && height > 0);
+    return launch_consistency(d_disparity, d_keys, width, height, d_checked,
+                              static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_median3_device(const float *d_image, uint32_t width, uint32_t height,
+                                         uint32_t stage_mask, float *d_filtered, void *stream) {
+    CHECK_SIZE(d_image && d_filtered && width > 0 && height > 0);
+    return launch_median3(d_image, width, height, stage_mask ? 1 : 0, d_filtered,
+                          static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+static Camera to_camera(const nxs_camera *c) {
+    Camera k;
+    memcpy(k.k, c->k, sizeof k.k);
+    memcpy(k.d, c->d, sizeof k.d);
+    memcpy(k.inverse_pr, c->inverse_pr, sizeof k.inverse_pr);
+    return k;
+}
+
+extern "C" nxs_status nxs_rectify_device(const uint8_t *d_frame, uint32_t frame_width,
+                                         uint32_t frame_height, const nxs_camera *camera,
+                                         uint32_t width, uint32_t height, uint8_t *d_rectified,
+                                         void *stream) {
+    CHECK_SIZE(d_frame && camera && d_rectified && width > 0 && height > 0 &&
+               frame_width >= width && frame_height >= height);
+    return launch_rectify(d_frame, frame_width, frame_height, to_camera(camera), width, height,
+                          d_rectified, static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_despeckle_device(const float *d_disparity, uint32_t width,
+                                           uint32_t height, float min_support, float max_diff,
+                                           uint32_t radius, float *d_despeckled, void *stream) {
+    CHECK_SIZE(d_disparity && d_despeckled && width > 0 && height > 0 && radius >= 1 &&
+               radius <= 8);
+    return launch_despeckle(d_disparity, width, height, min_support, max_diff, radius,
+                            d_despeckled, static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_temporal_device(float *d_disparity, float *d_previous, float *d_missed,
+                                          uint64_t pixels, float alpha, float delta, float hold,
+                                          float max_missed, void *stream) {
+    CHECK_SIZE(d_disparity && d_previous && d_missed);
+    if (pixels == 0) return NXS_OK;
+    return launch_temporal(d_disparity, d_previous, d_missed, pixels, alpha, delta, hold,
+                           max_missed, static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_depth_device(const float *d_disparity, uint64_t pixels,
+                                       float focal_length_px, float baseline_m,
+                                       uint16_t *d_depth_mm, float *d_depth_m, void *stream) {
+    CHECK_SIZE(d_disparity && d_depth_mm && d_depth_m);
+    if (pixels == 0) return NXS_OK;
+    return launch_depth(d_disparity, pixels, focal_length_px, baseline_m, d_depth_mm, d_depth_m,
+                        static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_cloud_device(const float *d_depth_m, uint32_t width, uint32_t height,
+                                       uint32_t decimation, float focal_length_px, float cx,
+                                       float cy, float nearest_m, float farthest_m,
+                                       float *d_grid, int32_t *d_kept, void *stream) {
+    CHECK_SIZE(d_depth_m && d_grid && d_kept && decimation >= 1 && decimation <= width &&
+               decimation <= height);
+    return launch_cloud(d_depth_m, width, height, decimation, focal_length_px, cx, cy, nearest_m,
+                        farthest_m, d_grid, d_kept, static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_quality_device(const float *d_disparity, float *d_previous,
+                                         uint32_t width, uint32_t height, float *d_sums,
+                                         void *stream) {
+    CHECK_SIZE(d_disparity && d_previous && d_sums && width > 0 && height > 0);
+    // The per-column sums live in a small stream-ordered allocation.
+    float *columns = nullptr;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (cudaMallocAsync(reinterpret_cast<void **>(&columns), sizeof(float) * 5 * width, s))
+        return NXS_CUDA_ERROR;
+    cudaError_t e = launch_quality(d_disparity, d_previous, width, height, columns, d_sums, s);
+    cudaFreeAsync(columns, s);
+    return e ? NXS_CUDA_ERROR : NXS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The segment protocol
+
+namespace {
+
+const char *kind_names[] = {"rectification", "disparity", "speckle_filter", "temporal_filter",
+                            "depth", "point_cloud", "quality"};
+
+bool parse_kind(const char *name, Kind *kind) {
+    for (int i = 0; i < 7; ++i)
+        if (name && strcmp(name, kind_names[i]) == 0) {
+            *kind = static_cast<Kind>(i);
+            return true;
+        }
+    return false;
+}
+
+std::vector<std::string> requires_of(Kind k) {
+    switch (k) {
+    case Kind::Rectification: return {"left_frame", "right_frame"};
+    case Kind::Disparity: return {"left", "right"};
+    case Kind::Cloud: return {"depth_m"};
+    default: return {"disparity"};
+    }
+}
+
+std::vector<std::string> provides_of(Kind k) {
+    switch (k) {
+    case Kind::Rectification: return {"left", "right"};
+    case Kind::Depth: return {"depth_mm", "depth_m"};
+    case Kind::Cloud: return {"cloud_grid", "cloud_points"};
+    case Kind::Quality: return {"quality_sums"};
+    default: return {"disparity"};
+    }
+}
+
+// The outputs a member returns (native/stereo_match/src/segment.rs:74-89):
+// depth_m stays on the device.
+std::vector<std::string> outputs_of(Kind k) {
+    switch (k) {
+    case Kind::Rectification: return {"left", "right"};
+    case Kind::Depth: return {"depth_mm"};
+    case Kind::Cloud: return {"cloud_grid", "cloud_points"};
+    case Kind::Quality: return {"quality_sums"};
+    default: return {"disparity"};
+    }
+}
+
+const nxs_setting *find_setting(const nxs_member &m, const char *name) {
+    for (uint32_t i = 0; i < m.n_settings; ++i)
+        if (m.settings[i].name && strcmp(m.settings[i].name, name) == 0) return &m.settings[i];
+    return nullptr;
+}
+
+// segment.rs:98-111: the settings a kind does not take, sorted.
+bool takes_only(const nxs_member &m, std::initializer_list<const char *> names,
+                std::string *why) {
+    std::vector<std::string> unknown;
+    for (uint32_t i = 0; i < m.n_settings; ++i) {
+        const char *n = m.settings[i].name ? m.settings[i].name : "";
+        bool known = false;
+        for (const char *k : names) known = known || strcmp(n, k) == 0;
+        if (!known) unknown.push_back(n);
+    }
+    if (unknown.empty()) return true;
+    std::sort(unknown.begin(), unknown.end());
+    *why = std::string(m.kind) + " has no setting ";
+    for (size_t i = 0; i < unknown.size(); ++i) *why += (i ? ", " : "") + unknown[i];
+    return false;
+}
+
+bool option(const nxs_member &m, const char *name, double *value, std::string *why) {
+    const nxs_setting *s = find_setting(m, name);
+    if (!s) {
+        *why = std::string(m.kind) + " needs its " + name + " setting";
+        return false;
+    }
+    *value = s->value;
+    return true;
+}
+
+bool count_option(const nxs_member &m, const char *name, long lowest, long highest, int *out,
+                  std::string *why) {
+    double v;
+    if (!option(m, name, &v, why)) return false;
+    if (std::floor(v) == v && v >= (double)lowest && v <= (double)highest) {
+        *out = (int)v;
+        return true;
+    }
+    char buf[256];
+    snprintf(buf, sizeof buf, "%s %s must be an integer from %ld to %ld, got %g", m.kind, name,
+             lowest, highest, v);
+    *why = buf;
+    return false;
+}
+
+bool integer_option(const nxs_member &m, const char *name, std::vector<int> allowed, int *out,
+                    std::string *why) {
+    double v;
+    if (!option(m, name, &v, why)) return false;
+    for (int a : allowed)
+        if ((double)a == v) {
+            *out = a;
+            return true;
+        }
+    std::string list;
+    for (size_t i = 0; i < allowed.size(); ++i)
+        list += (i ? ", " : "") + std::to_string(allowed[i]);
+    char buf[256];
+    snprintf(buf, sizeof buf, "%s %s must be one of [%s], got %g", m.kind, name, list.c_str(), v);
+    *why = buf;
+    return false;
+}
+
+// segment.rs:242-333: a stage of `kind` with exactly the settings it takes.
+bool build_member(const nxs_geometry &g, const nxs_member &m, Member *out, std::string *why) {
+    if (!parse_kind(m.kind, &out->kind)) {
+        *why = std::string("no native implementation of ") + (m.kind ? m.kind : "(null)");
+        return false;
+    }
+    out->kind_name = m.kind;
+    const long w = g.width, h = g.height;
+    switch (out->kind) {
+    case Kind::Rectification:
+        if (!takes_only(m, {}, why)) return false;
+        if (g.frame_width < g.width || g.frame_height < g.height) {
+            char buf[256];
+            snprintf(buf, sizeof buf,
+                     "rectification only shrinks: %ux%u frames are smaller than the %ux%u "
+                     "working size",
+                     g.frame_width, g.frame_height, g.width, g.height);
+            *why = buf;
+            return false;
+        }
+        return true;
+    case Kind::Disparity: {
+        if (!takes_only(m, {"num_disparities", "paths"}, why)) return false;
+        if (!integer_option(m, "num_disparities", {64, 96, 128, 192, 256}, &out->disparities,
+                            why) ||
+            !integer_option(m, "paths", {3, 8}, &out->paths, why))
+            return false;
+        nxs_sgm_params p{(uint32_t)out->disparities, (uint32_t)out->paths, 8, 64, 1.0f, 1};
+        char buf[256];
+        if (nxs_sgm_check(&p, g.width, g.height, buf, sizeof buf)) {
+            *why = buf;
+            return false;
+        }
+        return true;
+    }
+    case Kind::Speckle:
+        if (!takes_only(m, {"radius"}, why)) return false;
+        return count_option(m, "radius", 1, std::min<long>(8, std::min(w, h)), &out->radius, why);
+    case Kind::Temporal: {
+        if (!takes_only(m, {"max_missed"}, why)) return false;
+        double v;
+        if (!option(m, "max_missed", &v, why)) return false;
+        out->max_missed = (float)v;
+        return true;
+    }
+    case Kind::Depth:
+        return takes_only(m, {}, why);
+    case Kind::Cloud: {
+        if (!takes_only(m, {"decimation", "min_depth_m", "max_depth_m"}, why)) return false;
+        double lo, hi;
+        if (!count_option(m, "decimation", 1, std::min(w, h), &out->decimation, why) ||
+            !option(m, "min_depth_m", &lo, why) || !option(m, "max_depth_m", &hi, why))
+            return false;
+        out->min_depth_m = (float)lo;
+        out->max_depth_m = (float)hi;
+        return true;
+    }
+    case Kind::Quality:
+        return takes_only(m, {}, why);
+    }
+    return false;
+}
+
+Spec entry_spec(const std::string &name, const nxs_geometry &g, bool *ok) {
+    *ok = true;
+    if (name == "left_frame" || name == "right_frame")
+        return {name, NXS_U8, {g.frame_height, g.frame_width}};
+    if (name == "left" || name == "right") return {name, NXS_U8, {g.height, g.width}};
+    if (name == "disparity") return {name, NXS_F32, {g.height, g.width}};
+    *ok = false;
+    return {};
+}
+
+Spec output_spec(const std::string &name, const nxs_geometry &g, const Member &m) {
+    if (name == "left" || name == "right") return {name, NXS_U8, {g.height, g.width}};
+    if (name == "disparity") return {name, NXS_F32, {g.height, g.width}};
+    if (name == "depth_mm") return {name, NXS_U16, {g.height, g.width}};
+    if (name == "cloud_grid")
+        return {name, NXS_F32,
+                {g.height / (uint32_t)m.decimation, g.width / (uint32_t)m.decimation, 3}};
+    if (name == "cloud_points") return {name, NXS_S32, {}};
+    return {name, NXS_F32, {5}};  // quality_sums
+}
+
+const nxs_param *find_param(const nxs_member_params &mp, const char *name) {
+    for (uint32_t i = 0; i < mp.n_params; ++i)
+        if (mp.params[i].name && strcmp(mp.params[i].name, name) == 0) return &mp.params[i];
+    return nullptr;
+}
+
+// segment.rs:131-165: a live input of the right length.
+bool input(const nxs_member_params &mp, const char *name, uint32_t length, const float **values,
+           std::string *why) {
+    const nxs_param *p = find_param(mp, name);
+    if (!p) {
+        *why = std::string("no ") + name + " among the stage's inputs";
+        return false;
+    }
+    if (p->count != length || !p->values) {
+        *why = std::string(name) + " has " + std::to_string(p->count) + " values, expected " +
+               std::to_string(length);
+        return false;
+    }
+    *values = p->values;
+    return true;
+}
+
+bool scalar(const nxs_member_params &mp, const char *name, float *value, std::string *why) {
+    const float *v;
+    if (!input(mp, name, 1, &v, why)) return false;
+    *value = v[0];
+    return true;
+}
+
+bool penalty(const nxs_member_params &mp, const char *name, uint32_t *value, std::string *why) {
+    float v;
+    if (!scalar(mp, name, &v, why)) return false;
+    if (std::floor(v) == v && v >= 0.0f && v <= 255.0f) {
+        *value = (uint32_t)v;
+        return true;
+    }
+    char buf[128];
+    snprintf(buf, sizeof buf, "%s must be an integer from 0 to 255, got %g", name, (double)v);
+    *why = buf;
+    return false;
+}
+
+bool camera(const nxs_member_params &mp, const char *side, Camera *k, std::string *why) {
+    const float *v;
+    std::string s(side);
+    if (!input(mp, (s + ".k").c_str(), 9, &v, why)) return false;
+    memcpy(k->k, v, sizeof k->k);
+    if (!input(mp, (s + ".d").c_str(), 5, &v, why)) return false;
+    memcpy(k->d, v, sizeof k->d);
+    if (!input(mp, (s + ".inverse_pr").c_str(), 9, &v, why)) return false;
+    memcpy(k->inverse_pr, v, sizeof k->inverse_pr);
+    return true;
+}
+
+// Parsed live inputs of one member for one pair.
+struct Live {
+    Camera cameras[2];
+    nxs_sgm_params sgm{};
+    float a = 0, b = 0, c = 0;  // stage scalars
+};
+
+bool parse_live(const Member &m, const nxs_geometry &g, const nxs_member_params &mp, Live *live,
+                std::string *why) {
+    switch (m.kind) {
+    case Kind::Rectification:
+        return camera(mp, "left", &live->cameras[0], why) &&
+               camera(mp, "right", &live->cameras[1], why);
+    case Kind::Disparity: {
+        live->sgm.disparities = m.disparities;
+        live->sgm.paths = m.paths;
+        live->sgm.stage_mask = 1;
+        if (!penalty(mp, "p1", &live->sgm.p1, why) || !penalty(mp, "p2", &live->sgm.p2, why) ||
+            !scalar(mp, "uniqueness", &live->sgm.uniqueness, why))
+            return false;
+        char buf[256];
+        if (nxs_sgm_check(&live->sgm, g.width, g.height, buf, sizeof buf)) {
+            *why = buf;
+            return false;
+        }
+        return true;
+    }
+    case Kind::Speckle:
+        return scalar(mp, "min_support", &live->a, why) && scalar(mp, "max_diff", &live->b, why);
+    case Kind::Temporal:
+        return scalar(mp, "alpha", &live->a, why) && scalar(mp, "delta", &live->b, why) &&
+               scalar(mp, "hold", &live->c, why);
+    case Kind::Depth:
+        return scalar(mp, "focal_length_px", &live->a, why) &&
+               scalar(mp, "baseline_m", &live->b, why);
+    case Kind::Cloud:
+        return scalar(mp, "focal_length_px", &live->a, why) && scalar(mp, "cx", &live->b, why) &&
+               scalar(mp, "cy", &live->c, why);
+    case Kind::Quality:
+        return true;
+    }
+    return false;
+}
+
+}  // namespace
+
+extern "C" nxs_status nxs_configure(nxs_context *c, uint32_t id, const nxs_geometry *geometry,
+                                    uint32_t n_members, const nxs_member *members, char *error,
+                                    size_t error_len) {
+    if (!c || !geometry || (n_members && !members)) {
+        set_error(error, error_len, "a NULL context, geometry or member list");
+        return NXS_BAD_ARGUMENT;
+    }
+    const nxs_geometry g = *geometry;
+    if (g.width < 2 || g.height < 2 || g.width > 65535 || g.height > 65535) {
+        set_error(error, error_len, "a segment works at 2x2 or more, got %ux%u", g.width,
+                  g.height);
+        return NXS_REFUSED;
+    }
+    auto seg = std::make_shared<Segment>();
+    seg->id = id;
+    seg->device = c->device;
+    seg->g = g;
+    std::vector<std::string> provided;
+    for (uint32_t i = 0; i < n_members; ++i) {
+        Member m;
+        std::string why;
+        if (!build_member(g, members[i], &m, &why)) {
+            set_error(error, error_len, "%s", why.c_str());
+            return NXS_REFUSED;
+        }
+        for (const std::string &r : requires_of(m.kind)) {
+            bool have = std::find(provided.begin(), provided.end(), r) != provided.end();
+            bool listed = false;
+            for (const Spec &e : seg->entries) listed = listed || e.name == r;
+            if (have || listed) continue;
+            bool ok;
+            Spec spec = entry_spec(r, g, &ok);
+            if (!ok) {
+                set_error(error, error_len,
+                          "no stage before it provides %s, and a segment cannot take it as an "
+                          "entry",
+                          r.c_str());
+                return NXS_REFUSED;
+            }
+            seg->entries.push_back(spec);
+        }
+        for (const std::string &p : provides_of(m.kind)) provided.push_back(p);
+        for (const std::string &o : outputs_of(m.kind)) {
+            bool listed = false;
+            for (const Spec &e : seg->outputs) listed = listed || e.name == o;
+            if (!listed) seg->outputs.push_back(output_spec(o, g, m));
+        }
+        seg->members.push_back(m);
+    }
+    cudaSetDevice(c->device);
+    cudaError_t e = cudaStreamCreateWithFlags(&seg->stream, cudaStreamNonBlocking);
+    const size_t pixels = (size_t)g.width * g.height;
+    const size_t frame = (size_t)g.frame_width * g.frame_height;
+    int max_disparities = 0, decimation = 1;
+    for (const Member &m : seg->members) {
+        if (m.kind == Kind::Disparity) max_disparities = std::max(max_disparities, m.disparities);
+        if (m.kind == Kind::Cloud) decimation = m.decimation;
+    }
+    if (!e) e = seg->alloc(&seg->frames[0], std::max<size_t>(frame, 1));
+    if (!e) e = seg->alloc(&seg->frames[1], std::max<size_t>(frame, 1));
+    if (!e) e = seg->alloc(&seg->images[0], pixels);
+    if (!e) e = seg->alloc(&seg->images[1], pixels);
+    if (!e) e = seg->alloc(&seg->disparity[0], pixels);
+    if (!e) e = seg->alloc(&seg->disparity[1], pixels);
+    if (!e) e = seg->alloc(&seg->depth_m, pixels);
+    if (!e) e = seg->alloc(&seg->depth_mm, pixels);
+    if (!e) e = seg->alloc(&seg->grid, 3 * (pixels / (decimation * decimation) + 1));
+    if (!e) e = seg->alloc(&seg->kept, 1);
+    if (!e) e = seg->alloc(&seg->quality_sums, 5);
+    if (!e) e = seg->alloc(&seg->quality_columns, 5 * (size_t)g.width);
+    if (!e && max_disparities)
+        e = seg->scratch.reserve(matcher_scratch_bytes(g.width, g.height, max_disparities));
+    // What the stages carry starts over: previous = -1, missed = 0
+    // (stage/temporal_filter.ex:219-226, stage/quality.ex:144-145).
+    for (Member &m : seg->members) {
+        if (e) break;
+        if (m.kind == Kind::Temporal || m.kind == Kind::Quality) {
+            e = seg->alloc(&m.previous, pixels);
+            if (!e) {
+                std::vector<float> minus(pixels, -1.0f);
+                e = cudaMemcpy(m.previous, minus.data(), 4 * pixels, cudaMemcpyHostToDevice);
+            }
+        }
+        if (!e && m.kind == Kind::Temporal) {
+            e = seg->alloc(&m.missed, pixels);
+            if (!e) e = cudaMemset(m.missed, 0, 4 * pixels);
+        }
+    }
+    if (e) return cuda_status(e, error, error_len, "segment allocation");
+    std::lock_guard<std::mutex> lock(c->lock);
+    c->segments[id] = seg;  // replaces (and, once its requests finish, frees) an older one
+    return NXS_OK;
+}
+
+static void CUDART_CB request_done(void *data) {
+    nxs_request *r = static_cast<nxs_request *>(data);
+    if (r->callback) r->callback(r->user, r->tag);
+}
+
+extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_members,
+                                    const nxs_member_params *params, uint32_t n_entries,
+                                    const nxs_tensor *entries, nxs_done_fn done, void *user,
+                                    uint64_t tag, nxs_request **request, char *error,
+                                    size_t error_len) {
+    if (!c || !request || (n_members && !params) || (n_entries && !entries)) {
+        set_error(error, error_len, "a NULL context, request, params or entries");
+        return NXS_BAD_ARGUMENT;
+    }
+    *request = nullptr;
+    std::shared_ptr<Segment> seg;
+    {
+        std::lock_guard<std::mutex> lock(c->lock);
+        auto it = c->segments.find(id);
+        if (it == c->segments.end()) {
+            set_error(error, error_len, "no segment %u", id);
+            return NXS_NO_SEGMENT;
+        }
+        seg = it->second;
+    }
+    const nxs_geometry &g = seg->g;
+    if (n_members != seg->members.size()) {
+        set_error(error, error_len, "%zu stages, got the inputs of %u", seg->members.size(),
+                  n_members);
+        return NXS_BAD_RUN;
+    }
+    std::vector<Live> live(seg->members.size());
+    for (size_t i = 0; i < seg->members.size(); ++i) {
+        std::string why;
+        if (!parse_live(seg->members[i], g, params[i], &live[i], &why)) {
+            set_error(error, error_len, "%s", why.c_str());
+            return NXS_BAD_RUN;
+        }
+    }
+    // Match the entries to the segment's: name, type and shape.
+    std::vector<const nxs_tensor *> matched(seg->entries.size(), nullptr);
+    for (size_t k = 0; k < seg->entries.size(); ++k) {
+        const Spec &spec = seg->entries[k];
+        for (uint32_t i = 0; i < n_entries; ++i)
+            if (entries[i].name && spec.name == entries[i].name) matched[k] = &entries[i];
+        const nxs_tensor *t = matched[k];
+        if (!t) {
+            set_error(error, error_len, "missing entry %s", spec.name.c_str());
+            return NXS_BAD_RUN;
+        }
+        bool shape_ok = t->type == spec.type && t->rank == spec.dims.size();
+        for (size_t d = 0; shape_ok && d < spec.dims.size(); ++d)
+            shape_ok = t->dims[d] == spec.dims[d];
+        if (!shape_ok || !t->data || t->bytes != spec.bytes()) {
+            set_error(error, error_len, "entry %s: expected type %u of shape {%u, %u}, %zu bytes",
+                      spec.name.c_str(), spec.type, spec.dims[0], spec.dims[1], spec.bytes());
+            return NXS_BAD_RUN;
+        }
+    }
+
+    cudaSetDevice(c->device);
+    auto *r = new nxs_request();
+    r->segment = seg;
+    r->callback = done;
+    r->user = user;
+    r->tag = tag;
+    cudaError_t e = cudaSuccess;
+    const size_t n = seg->members.size();
+    r->marks.resize(n + 1, nullptr);
+    for (size_t i = 0; i <= n && !e; ++i) e = cudaEventCreate(&r->marks[i]);
+    if (!e) e = cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming);
+    // Stage the entries in pinned memory now: the caller's buffers are only
+    // borrowed for the call.
+    std::vector<void *> staged(seg->entries.size(), nullptr);
+    for (size_t k = 0; k < seg->entries.size() && !e; ++k) {
+        staged[k] = seg->pinned.take(seg->entries[k].bytes());
+        if (!staged[k]) e = cudaErrorMemoryAllocation;
+        else {
+            memcpy(staged[k], matched[k]->data, seg->entries[k].bytes());
+            r->pinned.push_back(staged[k]);
+        }
+    }
+    std::vector<void *> out_host(seg->outputs.size(), nullptr);
+    for (size_t k = 0; k < seg->outputs.size() && !e; ++k) {
+        out_host[k] = seg->pinned.take(std::max<size_t>(seg->outputs[k].bytes(), 4));
+        if (!out_host[k]) e = cudaErrorMemoryAllocation;
+        else r->pinned.push_back(out_host[k]);
+    }
+    if (e) {
+        nxs_request_free(r);
+        return cuda_status(e, error, error_len, "request set-up");
+    }
+
+    std::lock_guard<std::mutex> order(seg->order);
+    cudaStream_t s = seg->stream;
+    const size_t pixels = (size_t)g.width * g.height;
+    int current = 0;  // which disparity buffer holds the disparity so far
+    for (size_t k = 0; k < seg->entries.size() && !e; ++k) {
+        const std::string &name = seg->entries[k].name;
+        void *dst = name == "left_frame" ? (void *)seg->frames[0]
+                    : name == "right_frame" ? (void *)seg->frames[1]
+                    : name == "left"        ? (void *)seg->images[0]
+                    : name == "right"       ? (void *)seg->images[1]
+                                            : (void *)seg->disparity[0];
+        e = cudaMemcpyAsync(dst, staged[k], seg->entries[k].bytes(), cudaMemcpyHostToDevice, s);
+    }
+    for (size_t i = 0; i < n && !e; ++i) {
+        Member &m = seg->members[i];
+        const Live &l = live[i];
+        e = cudaEventRecord(r->marks[i], s);
+        if (e) break;
+        switch (m.kind) {
+        case Kind::Rectification:
+            for (int side = 0; side < 2 && !e; ++side)
+                e = launch_rectify(seg->frames[side], g.frame_width, g.frame_height,
+                                   l.cameras[side], g.width, g.height, seg->images[side], s);
+            break;
+        case Kind::Disparity: {
+            MatcherScratch ms =
+                carve_matcher_scratch(seg->scratch.ptr, g.width, g.height, m.disparities);
+            e = run_matcher(seg->images[0], seg->images[1], g.width, g.height, m.disparities,
+                            m.paths, l.sgm.p1, l.sgm.p2, l.sgm.uniqueness, 1, ms,
+                            seg->disparity[current], s);
+            break;
+        }
+        case Kind::Speckle:
+            e = launch_despeckle(seg->disparity[current], g.width, g.height, l.a, l.b, m.radius,
+                                 seg->disparity[1 - current], s);
+            current = 1 - current;
+            break;
+        case Kind::Temporal:
+            e = launch_temporal(seg->disparity[current], m.previous, m.missed, pixels, l.a, l.b,
+                                l.c, m.max_missed, s);
+            break;
+        case Kind::Depth:
+            e = launch_depth(seg->disparity[current], pixels, l.a, l.b, seg->depth_mm,
+                             seg->depth_m, s);
+            break;
+        case Kind::Cloud:
+            e = launch_cloud(seg->depth_m, g.width, g.height, m.decimation, l.a, l.b, l.c,
+                             m.min_depth_m, m.max_depth_m, seg->grid, seg->kept, s);
+            break;
+        case Kind::Quality:
+            e = launch_quality(seg->disparity[current], m.previous, g.width, g.height,
+                               seg->quality_columns, seg->quality_sums, s);
+            break;
+        }
+    }
+    if (!e) e = cudaEventRecord(r->marks[n], s);
+    // Download the outputs into the request's pinned blocks.
+    r->outputs.resize(seg->outputs.size());
+    r->names.resize(seg->outputs.size());
+    for (size_t k = 0; k < seg->outputs.size() && !e; ++k) {
+        const Spec &spec = seg->outputs[k];
+        const void *src = spec.name == "left"           ? (const void *)seg->images[0]
+                          : spec.name == "right"        ? (const void *)seg->images[1]
+                          : spec.name == "disparity"    ? (const void *)seg->disparity[current]
+                          : spec.name == "depth_mm"     ? (const void *)seg->depth_mm
+                          : spec.name == "cloud_grid"   ? (const void *)seg->grid
+                          : spec.name == "cloud_points" ? (const void *)seg->kept
+                                                        : (const void *)seg->quality_sums;
+        e = cudaMemcpyAsync(out_host[k], src, spec.bytes(), cudaMemcpyDeviceToHost, s);
+        r->names[k] = spec.name;
+        nxs_tensor &t = r->outputs[k];
+        t.name = r->names[k].c_str();
+        t.type = spec.type;
+        t.rank = (uint32_t)spec.dims.size();
+        for (size_t d = 0; d < 4; ++d) t.dims[d] = d < spec.dims.size() ? spec.dims[d] : 0;
+        t.data = out_host[k];
+        t.bytes = spec.bytes();
+    }
+    if (!e) e = cudaEventRecord(r->done, s);
+    if (!e && done) e = cudaLaunchHostFunc(s, request_done, r);
+    if (e) {
+        // The stream is still ordered: wait for what was enqueued before freeing.
+        cudaStreamSynchronize(s);
+        nxs_request_free(r);
+        return cuda_status(e, error, error_len, "enqueueing the request");
+    }
+    *request = r;
+    return NXS_OK;
+}
+
+extern "C" nxs_status nxs_request_poll(nxs_request *r, char *error, size_t error_len) {
+    if (!r) return NXS_BAD_ARGUMENT;
+    cudaSetDevice(r->segment->device);
+    cudaError_t e = cudaEventQuery(r->done);
+    if (e == cudaErrorNotReady) return NXS_PENDING;
+    return cuda_status(e, error, error_len, "request");
+}
+
+extern "C" nxs_status nxs_request_wait(nxs_request *r, int64_t timeout_ms, char *error,
+                                       size_t error_len) {
+    if (!r) return NXS_BAD_ARGUMENT;
+    cudaSetDevice(r->segment->device);
+    if (timeout_ms < 0) return cuda_status(cudaEventSynchronize(r->done), error, error_len, "request");
+    const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeout_ms);
+    int spins = 0;
+    for (;;) {
+        cudaError_t e = cudaEventQuery(r->done);
+        if (e != cudaErrorNotReady) return cuda_status(e, error, error_len, "request");
+        if (std::chrono::steady_clock::now() >= deadline) {
+            set_error(error, error_len, "timeout after %lld ms", (long long)timeout_ms);
+            return NXS_TIMEOUT;
+        }
+        if (++spins < 2000) std::this_thread::yield();
+        else std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+}
+
+extern "C" nxs_status nxs_request_outputs(nxs_request *r, uint32_t *n_outputs,
+                                          const nxs_tensor **outputs) {
+    if (!r || !n_outputs || !outputs) return NXS_BAD_ARGUMENT;
+    nxs_status s = nxs_request_poll(r, nullptr, 0);
+    if (s) return s;
+    *n_outputs = (uint32_t)r->outputs.size();
+    *outputs = r->outputs.data();
+    return NXS_OK;
+}
+
+extern "C" nxs_status nxs_request_times(nxs_request *r, uint32_t *n_members,
+                                        const uint32_t **times_us) {
+    if (!r || !n_members || !times_us) return NXS_BAD_ARGUMENT;
+    nxs_status s = nxs_request_poll(r, nullptr, 0);
+    if (s) return s;
+    if (!r->timed) {
+        r->times_us.clear();
+        for (size_t i = 0; i + 1 < r->marks.size(); ++i) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, r->marks[i], r->marks[i + 1]);
+            double us = std::round((double)ms * 1000.0);
+            r->times_us.push_back(us > 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)us);
+        }
+        r->timed = true;
+    }
+    *n_members = (uint32_t)r->times_us.size();
+    *times_us = r->times_us.data();
+    return NXS_OK;
+}
+
+extern "C" void nxs_request_free(nxs_request *r) {
+    if (!r) return;
+    cudaSetDevice(r->segment->device);
+    if (r->done) cudaEventSynchronize(r->done);
+    for (cudaEvent_t ev : r->marks)
+        if (ev) cudaEventDestroy(ev);
+    if (r->done) cudaEventDestroy(r->done);
+    for (void *p : r->pinned) r->segment->pinned.give(p);
+    delete r;
+}
+
+extern "C" nxs_status nxs_release(nxs_context *c, uint32_t id) {
+    if (!c) return NXS_BAD_ARGUMENT;
+    std::shared_ptr<Segment> seg;
+    {
+        std::lock_guard<std::mutex> lock(c->lock);
+        auto it = c->segments.find(id);
+        if (it == c->segments.end()) return NXS_NO_SEGMENT;
+        seg = it->second;
+        c->segments.erase(it);
+    }
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(seg->stream);
+    return NXS_OK;
+}

@@ -1,0 +1,83 @@
+// Launchers of the device kernels (one stream each, asynchronous). Sizes are
+// checked by the callers; each launcher returns cudaGetLastError().
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace nxs {
+
+// Directions in the reference's order (lib/nx_stereo.ex:566-570,
+// native/stereo_match/src/reference.rs:123-129).
+constexpr int kDirections[8][2] = {{0, 1}, {0, -1}, {1, 0}, {-1, 0},
+                                   {1, 1}, {1, -1}, {-1, 1}, {-1, -1}};
+
+struct Camera {
+    float k[9];
+    float d[5];
+    float inverse_pr[9];
+};
+
+// ---- the matcher ----
+// codes[image][y][x]: image 0 from `left`, 1 from `right` (right may be null
+// to run one image).
+cudaError_t launch_census(const uint8_t *left, const uint8_t *right, int width, int height,
+                          uint64_t *left_codes, uint64_t *right_codes, cudaStream_t stream);
+cudaError_t launch_costs(const uint64_t *left_codes, const uint64_t *right_codes, int width,
+                         int height, int disparities, uint8_t *costs, cudaStream_t stream);
+// paths_out[p][y][x][d] (u8) for p < paths.
+cudaError_t launch_paths(const uint8_t *costs, int width, int height, int disparities, int paths,
+                         int p1, int p2, uint8_t *paths_out, cudaStream_t stream);
+// sums[y][x][d] = sum over paths of paths_in (u16).
+cudaError_t launch_sum_paths(const uint8_t *paths_in, int width, int height, int disparities,
+                             int paths, uint16_t *sums, cudaStream_t stream);
+cudaError_t launch_select_paths(const uint8_t *paths_in, int width, int height, int disparities,
+                                int paths, float uniqueness, float *disparity, uint32_t *keys,
+                                cudaStream_t stream);
+cudaError_t launch_select_sums(const uint16_t *sums, int width, int height, int disparities,
+                               float uniqueness, float *disparity, uint32_t *keys,
+                               cudaStream_t stream);
+cudaError_t launch_consistency(const float *disparity, const uint32_t *keys, int width,
+                               int height, float *checked, cudaStream_t stream);
+cudaError_t launch_median3(const float *image, int width, int height, int stage_mask,
+                           float *filtered, cudaStream_t stream);
+
+// ---- the stages around it ----
+cudaError_t launch_rectify(const uint8_t *frame, int frame_width, int frame_height,
+                           const Camera &camera, int width, int height, uint8_t *rectified,
+                           cudaStream_t stream);
+cudaError_t launch_despeckle(const float *disparity, int width, int height, float min_support,
+                             float max_diff, int radius, float *despeckled, cudaStream_t stream);
+cudaError_t launch_temporal(float *disparity, float *previous, float *missed, size_t pixels,
+                            float alpha, float delta, float hold, float max_missed,
+                            cudaStream_t stream);
+cudaError_t launch_depth(const float *disparity, size_t pixels, float focal_length_px,
+                         float baseline_m, uint16_t *depth_mm, float *depth_m,
+                         cudaStream_t stream);
+cudaError_t launch_cloud(const float *depth_m, int width, int height, int decimation,
+                         float focal_length_px, float cx, float cy, float nearest_m,
+                         float farthest_m, float *grid, int32_t *kept, cudaStream_t stream);
+// column_sums: scratch of 5 * width floats.
+cudaError_t launch_quality(const float *disparity, float *previous, int width, int height,
+                           float *column_sums, float *sums, cudaStream_t stream);
+
+// The matcher's device scratch for one pair, and its layout.
+struct MatcherScratch {
+    uint64_t *left_codes, *right_codes;
+    uint8_t *costs;
+    uint8_t *paths;
+    float *selected, *checked;
+    uint32_t *keys;
+};
+size_t matcher_scratch_bytes(int width, int height, int disparities);
+MatcherScratch carve_matcher_scratch(void *base, int width, int height, int disparities);
+
+// The whole matcher on device buffers: census, costs, paths, selection, the
+// check and the median (with Stage.Disparity's mask when stage_mask).
+cudaError_t run_matcher(const uint8_t *left, const uint8_t *right, int width, int height,
+                        int disparities, int paths, int p1, int p2, float uniqueness,
+                        int stage_mask, const MatcherScratch &scratch, float *disparity,
+                        cudaStream_t stream);
+
+}  // namespace nxs

@@ -1,0 +1,264 @@
+// The stages around the matcher: Stage.Rectification, Stage.SpeckleFilter,
+// Stage.TemporalFilter, Stage.Depth, Stage.PointCloud and Stage.Quality.
+// Every f32 step is rounded on its own in the reference's order (the Nx
+// evaluator's, which the reference's native stages reproduce), so integer
+// outputs (rectified images, depth_mm) are bit-exact.
+#include "nxs_device.cuh"
+#include "nxs_kernels.h"
+
+namespace nxs {
+
+// ---------------------------------------------------------------- rectify
+// lib/nx_stereo/rectify.ex:133-207: the rectified pixel (u, v) projects into
+// the frame through inverse_pr, plumb_bob distortion (the radial polynomial
+// summed as 1 + (k3 r2^3 + (k2 r2^2 + k1 r2)), the order of Nx's expression,
+// native/stereo_match/src/rectify.rs:116-121) and the camera matrix; it is
+// scaled to the frame size at pixel centres and sampled bilinearly with 0
+// outside, then rounded half away from zero and clipped to u8.
+__global__ void rectify_kernel(const uint8_t *__restrict__ frame, int frame_width,
+                               int frame_height, const Camera camera, float scale_x,
+                               float scale_y, int width, uint8_t *__restrict__ rectified) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = blockIdx.y;
+    if (u >= width) return;
+    const float uf = (float)u, vf = (float)v;
+    const float *ir = camera.inverse_pr;
+    float x = fadd(fadd(fmul(ir[0], uf), fmul(ir[1], vf)), ir[2]);
+    float y = fadd(fadd(fmul(ir[3], uf), fmul(ir[4], vf)), ir[5]);
+    const float w = fadd(fadd(fmul(ir[6], uf), fmul(ir[7], vf)), ir[8]);
+    x = fdiv(x, w);
+    y = fdiv(y, w);
+    const float k1 = camera.d[0], k2 = camera.d[1], t1 = camera.d[2], t2 = camera.d[3],
+                k3 = camera.d[4];
+    const float r2 = fadd(fmul(x, x), fmul(y, y));
+    const float cubic = fmul(fmul(fmul(k3, r2), r2), r2);
+    const float square = fmul(fmul(k2, r2), r2);
+    const float radial = fadd(1.0f, fadd(cubic, fadd(square, fmul(k1, r2))));
+    const float xd = fadd(fadd(fmul(x, radial), fmul(fmul(fmul(2.0f, t1), x), y)),
+                          fmul(t2, fadd(r2, fmul(fmul(2.0f, x), x))));
+    const float yd = fadd(fadd(fmul(y, radial), fmul(t1, fadd(r2, fmul(fmul(2.0f, y), y)))),
+                          fmul(fmul(fmul(2.0f, t2), x), y));
+    const float *k = camera.k;
+    const float map_x = fadd(fadd(fmul(k[0], xd), fmul(k[1], yd)), k[2]);
+    const float map_y = fadd(fmul(k[4], yd), k[5]);
+    const float source_x = fsub(fmul(fadd(map_x, 0.5f), scale_x), 0.5f);
+    const float source_y = fsub(fmul(fadd(map_y, 0.5f), scale_y), 0.5f);
+    const float fx0 = floorf(source_x), fy0 = floorf(source_y);
+    const float wx = fsub(source_x, fx0), wy = fsub(source_y, fy0);
+    // float -> int as the reference casts: saturating, NaN to 0.
+    const int x0 = __float2int_rz(fx0), y0 = __float2int_rz(fy0);
+    float corner[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int sx = x0 + (i & 1), sy = y0 + (i >> 1);
+        const bool inside = sx >= 0 && sx < frame_width && sy >= 0 && sy < frame_height;
+        corner[i] = inside ? (float)__ldg(frame + (size_t)sy * frame_width + sx) : 0.0f;
+    }
+    const float top = fadd(fmul(fsub(1.0f, wx), corner[0]), fmul(wx, corner[1]));
+    const float bottom = fadd(fmul(fsub(1.0f, wx), corner[2]), fmul(wx, corner[3]));
+    const float value = fadd(fmul(fsub(1.0f, wy), top), fmul(wy, bottom));
+    float r = roundf(value);
+    r = r < 0.0f ? 0.0f : (r > 255.0f ? 255.0f : r);
+    rectified[(size_t)v * width + u] = (uint8_t)r;
+}
+
+cudaError_t launch_rectify(const uint8_t *frame, int frame_width, int frame_height,
+                           const Camera &camera, int width, int height, uint8_t *rectified,
+                           cudaStream_t stream) {
+    // Scale as the reference computes it: an f64 ratio rounded to f32.
+    const float scale_x = (float)((double)frame_width / (double)width);
+    const float scale_y = (float)((double)frame_height / (double)height);
+    dim3 grid((width + 127) / 128, height);
+    rectify_kernel<<<grid, 128, 0, stream>>>(frame, frame_width, frame_height, camera, scale_x,
+                                             scale_y, width, rectified);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- despeckle
+// lib/nx_stereo/filter.ex:47-80: support = the neighbours in the
+// (2r+1)^2 window, centre excluded, with n > 0 and |n - c| <= max_diff
+// (-1 outside the image); keep c where c > 0 and support >= min_support.
+// A 32x8 block stages its window in shared memory.
+constexpr int kSpeckleX = 32, kSpeckleY = 8;
+
+__global__ void __launch_bounds__(kSpeckleX *kSpeckleY)
+    despeckle_kernel(const float *__restrict__ disparity, int width, int height,
+                     float min_support, float max_diff, int radius,
+                     float *__restrict__ despeckled) {
+    extern __shared__ float window[];
+    const int tw = kSpeckleX + 2 * radius, th = kSpeckleY + 2 * radius;
+    const int x0 = blockIdx.x * kSpeckleX, y0 = blockIdx.y * kSpeckleY;
+    const int tid = threadIdx.y * kSpeckleX + threadIdx.x;
+    for (int i = tid; i < tw * th; i += kSpeckleX * kSpeckleY) {
+        int sy = y0 + i / tw - radius, sx = x0 + i % tw - radius;
+        window[i] = (sy >= 0 && sy < height && sx >= 0 && sx < width)
+                        ? disparity[(size_t)sy * width + sx]
+                        : -1.0f;
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    if (x >= width || y >= height) return;
+    const float centre = window[(threadIdx.y + radius) * tw + threadIdx.x + radius];
+    unsigned support = 0;
+    for (int dy = 0; dy <= 2 * radius; ++dy)
+        for (int dx = 0; dx <= 2 * radius; ++dx) {
+            if (dy == radius && dx == radius) continue;
+            const float n = window[(threadIdx.y + dy) * tw + threadIdx.x + dx];
+            support += (n > 0.0f) & (fabsf(fsub(n, centre)) <= max_diff);
+        }
+    const bool kept = centre > 0.0f && (float)support >= min_support;
+    despeckled[(size_t)y * width + x] = kept ? centre : -1.0f;
+}
+
+cudaError_t launch_despeckle(const float *disparity, int width, int height, float min_support,
+                             float max_diff, int radius, float *despeckled, cudaStream_t stream) {
+    dim3 block(kSpeckleX, kSpeckleY);
+    dim3 grid((width + kSpeckleX - 1) / kSpeckleX, (height + kSpeckleY - 1) / kSpeckleY);
+    size_t shared = sizeof(float) * (kSpeckleX + 2 * radius) * (kSpeckleY + 2 * radius);
+    despeckle_kernel<<<grid, block, shared, stream>>>(disparity, width, height, min_support,
+                                                      max_diff, radius, despeckled);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- temporal
+// lib/nx_stereo/filter.ex:122-130, in place over disparity, previous, missed.
+__global__ void temporal_kernel(float *__restrict__ disparity, float *__restrict__ previous,
+                                float *__restrict__ missed, size_t pixels, float alpha,
+                                float delta, float hold, float max_missed) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixels) return;
+    const float current = disparity[i], before = previous[i];
+    const bool matched = current > 0.0f;
+    const bool agree = matched && before > 0.0f && fabsf(fsub(current, before)) <= delta;
+    const float smoothed =
+        agree ? fadd(fmul(alpha, current), fmul(fsub(1.0f, alpha), before)) : current;
+    const float pairs_missed = matched ? 0.0f : fadd(missed[i], 1.0f);
+    const bool held = !matched && before > 0.0f && pairs_missed <= hold;
+    const float filtered = held ? before : smoothed;
+    disparity[i] = filtered;
+    previous[i] = filtered;
+    missed[i] = pairs_missed < max_missed ? pairs_missed : max_missed;
+}
+
+cudaError_t launch_temporal(float *disparity, float *previous, float *missed, size_t pixels,
+                            float alpha, float delta, float hold, float max_missed,
+                            cudaStream_t stream) {
+    temporal_kernel<<<(unsigned)((pixels + 255) / 256), 256, 0, stream>>>(
+        disparity, previous, missed, pixels, alpha, delta, hold, max_missed);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- depth
+// lib/nx_stereo/depth.ex:26-32: depth_m = (f * B) / d where d > 0, else 0;
+// depth_mm = round(depth_m * 1000), 0 beyond 65535.
+__global__ void depth_kernel(const float *__restrict__ disparity, size_t pixels,
+                             float focal_length_px, float baseline_m,
+                             uint16_t *__restrict__ depth_mm, float *__restrict__ depth_m) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixels) return;
+    const float focal_baseline = fmul(focal_length_px, baseline_m);
+    const float d = disparity[i];
+    const float metres = d > 0.0f ? fdiv(focal_baseline, d) : 0.0f;
+    const float rounded = roundf(fmul(metres, 1000.0f));
+    depth_m[i] = metres;
+    depth_mm[i] = rounded > 65535.0f ? 0 : (uint16_t)(rounded > 0.0f ? rounded : 0.0f);
+}
+
+cudaError_t launch_depth(const float *disparity, size_t pixels, float focal_length_px,
+                         float baseline_m, uint16_t *depth_mm, float *depth_m,
+                         cudaStream_t stream) {
+    depth_kernel<<<(unsigned)((pixels + 255) / 256), 256, 0, stream>>>(
+        disparity, pixels, focal_length_px, baseline_m, depth_mm, depth_m);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- cloud
+// lib/nx_stereo/depth.ex:73-89: point (i, j) from pixel (i*dec, j*dec),
+// x = (u - cx) * (z / f), y = (v - cy) * (z / f), NaN outside (near, far).
+__global__ void cloud_kernel(const float *__restrict__ depth_m, int width, int grid_width,
+                             int grid_height, int decimation, float focal_length_px, float cx,
+                             float cy, float nearest_m, float farthest_m,
+                             float *__restrict__ grid, int32_t *__restrict__ kept) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = blockIdx.y;
+    if (col >= grid_width || row >= grid_height) return;
+    const int x = col * decimation, y = row * decimation;
+    const float z = depth_m[(size_t)y * width + x];
+    float *point = grid + 3 * ((size_t)row * grid_width + col);
+    const bool in_range = z > nearest_m && z < farthest_m;
+    if (in_range) {
+        const float z_over_f = fdiv(z, focal_length_px);
+        point[0] = fmul(fsub((float)x, cx), z_over_f);
+        point[1] = fmul(fsub((float)y, cy), z_over_f);
+        point[2] = z;
+    } else {
+        point[0] = point[1] = point[2] = __int_as_float(0x7FC00000);
+    }
+    const unsigned ballot = __ballot_sync(__activemask(), in_range);
+    if ((threadIdx.x & 31) == __ffs(__activemask()) - 1 && ballot)
+        atomicAdd(kept, (int32_t)__popc(ballot));
+}
+
+cudaError_t launch_cloud(const float *depth_m, int width, int height, int decimation,
+                         float focal_length_px, float cx, float cy, float nearest_m,
+                         float farthest_m, float *grid, int32_t *kept, cudaStream_t stream) {
+    const int gw = width / decimation, gh = height / decimation;
+    cudaError_t e = cudaMemsetAsync(kept, 0, sizeof(int32_t), stream);
+    if (e) return e;
+    if (gw == 0 || gh == 0) return cudaSuccess;
+    dim3 grid_dim((gw + 127) / 128, gh);
+    cloud_kernel<<<grid_dim, 128, 0, stream>>>(depth_m, width, gw, gh, decimation,
+                                               focal_length_px, cx, cy, nearest_m, farthest_m,
+                                               grid, kept);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- quality
+// lib/nx_stereo/diagnostics.ex:264-271 with the native reduction order
+// (native/stereo_match/src/measures.rs:278-309): per column, the five planes
+// [matched, value, value^2, both, |change| * both] summed down the rows in
+// f64 and rounded to f32; then the columns summed in order in f64 and
+// rounded. One thread per column, then one per plane.
+__global__ void quality_columns_kernel(const float *__restrict__ disparity,
+                                       const float *__restrict__ previous, int width, int height,
+                                       float *__restrict__ column_sums) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= width) return;
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int y = 0; y < height; ++y) {
+        const float current = disparity[(size_t)y * width + x];
+        const float before = previous[(size_t)y * width + x];
+        const float matched = current > 0.0f ? 1.0f : 0.0f;
+        const float both = fmul(before > 0.0f ? 1.0f : 0.0f, matched);
+        const float value = fmul(current, matched);
+        acc[0] += (double)matched;
+        acc[1] += (double)value;
+        acc[2] += (double)fmul(value, value);
+        acc[3] += (double)both;
+        acc[4] += (double)fmul(fabsf(fsub(current, before)), both);
+    }
+#pragma unroll
+    for (int p = 0; p < 5; ++p) column_sums[(size_t)p * width + x] = (float)acc[p];
+}
+
+__global__ void quality_total_kernel(const float *__restrict__ column_sums, int width,
+                                     float *__restrict__ sums) {
+    const int p = threadIdx.x;
+    if (p >= 5) return;
+    double total = 0.0;
+    for (int x = 0; x < width; ++x) total += (double)column_sums[(size_t)p * width + x];
+    sums[p] = (float)total;
+}
+
+cudaError_t launch_quality(const float *disparity, float *previous, int width, int height,
+                           float *column_sums, float *sums, cudaStream_t stream) {
+    quality_columns_kernel<<<(width + 127) / 128, 128, 0, stream>>>(disparity, previous, width,
+                                                                    height, column_sums);
+    quality_total_kernel<<<1, 32, 0, stream>>>(column_sums, width, sums);
+    cudaError_t e = cudaGetLastError();
+    if (e) return e;
+    return cudaMemcpyAsync(previous, disparity, sizeof(float) * (size_t)width * height,
+                           cudaMemcpyDeviceToDevice, stream);
+}
+
+}  // namespace nxs

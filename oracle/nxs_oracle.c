@@ -316,7 +316,7 @@ void oracle_rectify(const uint8_t *frame, int frame_width, int frame_height,
 
 /* Keeps a matched pixel where at least min_support of the others in its
  * (2r+1)^2 window matched within max_diff of it; unmatched outside the image.
- * lib/nx_stereo/filter.ex:313-346, native/stereo_match/src/filters.rs:222-268. */
+ * lib/nx_stereo/filter.ex:47-80, native/stereo_match/src/filters.rs:222-268. */
 void oracle_despeckle(const float *disparity, int width, int height, float min_support,
                       float max_diff, int radius, float *despeckled) {
     for (int y = 0; y < height; ++y)
@@ -338,7 +338,7 @@ void oracle_despeckle(const float *disparity, int width, int height, float min_s
 }
 
 /* One step of the temporal filter, in place over disparity, previous and
- * missed. lib/nx_stereo/filter.ex:388-396, native/stereo_match/src/filters.rs:507-530. */
+ * missed. lib/nx_stereo/filter.ex:122-130, native/stereo_match/src/filters.rs:507-530. */
 void oracle_temporal(float *disparity, float *previous, float *missed, size_t pixels,
                      float alpha, float delta, float hold, float max_missed) {
     for (size_t i = 0; i < pixels; ++i) {
@@ -356,7 +356,7 @@ void oracle_temporal(float *disparity, float *previous, float *missed, size_t pi
 }
 
 /* depth_m = (f * B) / d where matched, else 0; depth_mm the rounded
- * millimetres, 0 beyond 65535. lib/nx_stereo/depth.ex:274-280,
+ * millimetres, 0 beyond 65535. lib/nx_stereo/depth.ex:26-32,
  * native/stereo_match/src/depth.rs:12-44. */
 void oracle_depth(const float *disparity, size_t pixels, float focal_length_px,
                   float baseline_m, uint16_t *depth_mm, float *depth_m) {

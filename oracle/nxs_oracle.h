@@ -89,6 +89,21 @@ int oracle_fast_sgm_batch(const uint8_t *lefts, const uint8_t *rights, int pairs
                           int height, int disparities, int paths, int p1, int p2,
                           float uniqueness, float *disparities_out, int threads);
 
+/* The full frame-to-depth chain per pair (rectification of both frames, the
+ * matcher with Stage.Disparity's mask, despeckle, depth, point cloud) on
+ * `threads` threads, a whole pair per thread at a time. Frames are pair-major
+ * [pairs][frame_height][frame_width]; disparities_out [pairs][height][width]
+ * (may be NULL). Returns the total of kept cloud points, or -1. */
+long oracle_fast_pipeline_batch(const uint8_t *left_frames, const uint8_t *right_frames,
+                                int pairs, int frame_width, int frame_height,
+                                const oracle_camera *left_camera,
+                                const oracle_camera *right_camera, int width, int height,
+                                int disparities, int paths, int p1, int p2, float uniqueness,
+                                float min_support, float max_diff, float focal_length_px,
+                                float baseline_m, int decimation, float cx, float cy,
+                                float nearest_m, float farthest_m, float *disparities_out,
+                                int threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -379,3 +379,85 @@ int oracle_fast_sgm_batch(const uint8_t *lefts, const uint8_t *rights, int pairs
     free(ids);
     return atomic_load(&b.failed) ? -1 : 0;
 }
+
+typedef struct {
+    const uint8_t *lefts, *rights;
+    int pairs, fw, fh, width, height, D, paths, p1, p2, decimation;
+    const oracle_camera *cameras[2];
+    float uniqueness, min_support, max_diff, focal, baseline, cx, cy, nearest, farthest;
+    float *outputs;
+    atomic_int next;
+    atomic_long kept;
+    atomic_int failed;
+} pipeline_t;
+
+static void *pipeline_worker(void *arg) {
+    pipeline_t *b = (pipeline_t *)arg;
+    scratch_t s;
+    size_t pixels = (size_t)b->width * b->height, frame = (size_t)b->fw * b->fh;
+    uint8_t *images = malloc(2 * pixels);
+    float *disparity = malloc(4 * pixels), *speckled = malloc(4 * pixels);
+    float *depth_m = malloc(4 * pixels);
+    uint16_t *depth_mm = malloc(2 * pixels);
+    int gw = b->width / b->decimation, gh = b->height / b->decimation;
+    float *grid = malloc(sizeof(float) * 3 * ((size_t)gw * gh + 1));
+    if (scratch_init(&s, b->width, b->height, b->D) || !images || !disparity || !speckled ||
+        !depth_m || !depth_mm || !grid) {
+        atomic_store(&b->failed, 1);
+    } else {
+        for (;;) {
+            int i = atomic_fetch_add(&b->next, 1);
+            if (i >= b->pairs) break;
+            oracle_rectify(b->lefts + i * frame, b->fw, b->fh, b->cameras[0], b->width,
+                           b->height, images);
+            oracle_rectify(b->rights + i * frame, b->fw, b->fh, b->cameras[1], b->width,
+                           b->height, images + pixels);
+            run_pair(&s, images, images + pixels, b->paths, b->p1, b->p2, b->uniqueness,
+                     disparity);
+            for (size_t k = 0; k < pixels; ++k)
+                if (!(disparity[k] > 0.0f)) disparity[k] = -1.0f;
+            oracle_despeckle(disparity, b->width, b->height, b->min_support, b->max_diff, 3,
+                             speckled);
+            oracle_depth(speckled, pixels, b->focal, b->baseline, depth_mm, depth_m);
+            long kept = oracle_cloud(depth_m, b->width, b->height, b->decimation, b->focal,
+                                     b->cx, b->cy, b->nearest, b->farthest, grid);
+            atomic_fetch_add(&b->kept, kept);
+            if (b->outputs) memcpy(b->outputs + i * pixels, speckled, 4 * pixels);
+        }
+    }
+    scratch_free(&s);
+    free(images); free(disparity); free(speckled); free(depth_m); free(depth_mm); free(grid);
+    return NULL;
+}
+
+long oracle_fast_pipeline_batch(const uint8_t *left_frames, const uint8_t *right_frames,
+                                int pairs, int frame_width, int frame_height,
+                                const oracle_camera *left_camera,
+                                const oracle_camera *right_camera, int width, int height,
+                                int disparities, int paths, int p1, int p2, float uniqueness,
+                                float min_support, float max_diff, float focal_length_px,
+                                float baseline_m, int decimation, float cx, float cy,
+                                float nearest_m, float farthest_m, float *disparities_out,
+                                int threads) {
+    if (refused(width, height, disparities, paths, p1, p2) || pairs < 0 || decimation < 1)
+        return -1;
+    if (threads < 1) threads = 1;
+    if (threads > pairs) threads = pairs > 0 ? pairs : 1;
+    pipeline_t b;
+    memset(&b, 0, sizeof b);
+    b.lefts = left_frames; b.rights = right_frames; b.pairs = pairs;
+    b.fw = frame_width; b.fh = frame_height; b.width = width; b.height = height;
+    b.D = disparities; b.paths = paths; b.p1 = p1; b.p2 = p2; b.decimation = decimation;
+    b.cameras[0] = left_camera; b.cameras[1] = right_camera;
+    b.uniqueness = uniqueness; b.min_support = min_support; b.max_diff = max_diff;
+    b.focal = focal_length_px; b.baseline = baseline_m; b.cx = cx; b.cy = cy;
+    b.nearest = nearest_m; b.farthest = farthest_m; b.outputs = disparities_out;
+    atomic_init(&b.next, 0);
+    atomic_init(&b.kept, 0);
+    atomic_init(&b.failed, 0);
+    pthread_t *ids = (pthread_t *)malloc(sizeof(pthread_t) * threads);
+    for (int t = 0; t < threads; ++t) pthread_create(&ids[t], NULL, pipeline_worker, &b);
+    for (int t = 0; t < threads; ++t) pthread_join(ids[t], NULL);
+    free(ids);
+    return atomic_load(&b.failed) ? -1 : atomic_load(&b.kept);
+}

@@ -52,6 +52,9 @@ def lib():
             "oracle_scene": (None, [_i, _i, ctypes.c_uint64, _u8p, _u8p]),
             "oracle_fast_sgm": (_i, [_u8p, _u8p, _i, _i, _i, _i, _i, _i, _f, _f32p]),
             "oracle_fast_sgm_batch": (_i, [_u8p, _u8p, _i, _i, _i, _i, _i, _i, _i, _f, _f32p, _i]),
+            "oracle_fast_pipeline_batch": (ctypes.c_long, [
+                _u8p, _u8p, _i, _i, _i, ctypes.POINTER(Camera), ctypes.POINTER(Camera), _i, _i,
+                _i, _i, _i, _i, _f, _f, _f, _f, _f, _i, _f, _f, _f, _f, ctypes.c_void_p, _i]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -232,3 +235,25 @@ def scene(width, height, seed):
     right = np.empty((height, width), np.uint8)
     lib().oracle_scene(width, height, seed, left, right)
     return left, right
+
+
+def fast_pipeline_batch(left_frames, right_frames, left_camera, right_camera, size,
+                        disparities=128, paths=8, p1=8, p2=64, uniqueness=1.0526315789473684,
+                        min_support=12.0, max_diff=1.0, focal_length_px=873.0, baseline_m=0.2,
+                        decimation=4, principal_point=(364.0, 272.0), nearest_m=0.05,
+                        farthest_m=20.0, threads=1, keep_disparities=False):
+    """Rectification, matcher, despeckle, depth and cloud per pair on `threads`
+    threads. Returns (kept points, disparities or None)."""
+    lefts = _c(left_frames, np.uint8)
+    rights = _c(right_frames, np.uint8)
+    n, fh, fw = lefts.shape
+    h, w = size
+    out = np.empty((n, h, w), np.float32) if keep_disparities else None
+    kept = lib().oracle_fast_pipeline_batch(
+        lefts, rights, n, fw, fh, ctypes.byref(left_camera), ctypes.byref(right_camera), w, h,
+        disparities, paths, p1, p2, uniqueness, min_support, max_diff, focal_length_px,
+        baseline_m, decimation, principal_point[0], principal_point[1], nearest_m, farthest_m,
+        out.ctypes.data if out is not None else None, threads)
+    if kept < 0:
+        raise ValueError("refused")
+    return int(kept), out
