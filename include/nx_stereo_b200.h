@@ -197,6 +197,23 @@ nxs_status nxs_sgm_device(nxs_context *context, const uint8_t *d_left, const uin
                           uint32_t width, uint32_t height, const nxs_sgm_params *params,
                           float *d_disparity, void *stream, char *error, size_t error_len);
 
+/* nxs_sgm_device for callers that must not allocate device memory: no
+ * counterpart in the reference (whose Rust matcher keeps its buffers in host
+ * memory). Callers whose device memory belongs to another allocator, or that
+ * cannot afford cudaMalloc's device synchronisation on their thread, pass only
+ * their inputs and outputs; the matcher's scratch is one fixed 64 MiB array in
+ * the library, held on every device that loads it until the process exits.
+ * Pairs needing more scratch than that (nxs_sgm_scratch_bytes; about 7 million
+ * pixel-disparities, e.g. 364x272 at 64) are refused with NXS_BAD_ARGUMENT.
+ * The first call on a device finds the array's device address (and loads it
+ * there); make that first call before any stream capture. All calls on a
+ * device share the array: calls that overlap on the device race, so the
+ * caller serialises them. No context is needed and none is used. */
+nxs_status nxs_sgm_device_static(const uint8_t *d_left, const uint8_t *d_right, uint32_t width,
+                                 uint32_t height, const nxs_sgm_params *params,
+                                 float *d_disparity, void *stream, char *error,
+                                 size_t error_len);
+
 /* The matcher's device scratch, in bytes, for one pair of this size. */
 uint64_t nxs_sgm_scratch_bytes(uint32_t width, uint32_t height, uint32_t disparities);
 
