@@ -32,7 +32,7 @@ import numpy as np  # noqa: E402
 METRIC = "pairs/s at 728x544x128 d, 8 paths (full frame-to-depth pipeline)"
 WIDTH, HEIGHT, DISPARITIES, PATHS = 728, 544, 128, 8
 DECIMATION = 4
-KERNELS_PER_STEP = 11  # rectify x2, census, costs, paths, select, check, median, despeckle, depth, cloud
+KERNELS_PER_STEP = 12  # rectify x2, census x2, costs, paths, select, check, median, despeckle, depth, cloud
 
 
 def parse():
@@ -157,38 +157,54 @@ class DevicePipeline:
                                 device=dev)
         self.kept = torch.empty(1, dtype=torch.int32, device=dev)
 
-    def step(self, frames, paths_events=None):
-        n, s, call = self.native, self.stream, self.native.call
+    STAGES = ["rectify", "census", "costs", "paths", "select", "consistency", "median",
+              "despeckle", "depth", "cloud"]
+
+    def step(self, frames, marks=None):
+        """One pair; `marks` (len(STAGES) + 1 CUDA events) bracket the stages."""
         import ctypes
 
+        s, call = self.stream, self.native.call
+
+        def mark(i):
+            if marks is not None:
+                marks[i].record()
+
+        mark(0)
         for side in range(2):
             call("nxs_rectify_device", frames[side].data_ptr(), WIDTH, HEIGHT,
                  ctypes.byref(self.cameras[side]), WIDTH, HEIGHT,
                  self.images[side].data_ptr(), s)
+        mark(1)
         call("nxs_census_device", self.images[0].data_ptr(), WIDTH, HEIGHT,
              self.codes[0].data_ptr(), s)
         call("nxs_census_device", self.images[1].data_ptr(), WIDTH, HEIGHT,
              self.codes[1].data_ptr(), s)
+        mark(2)
         call("nxs_costs_device", self.codes[0].data_ptr(), self.codes[1].data_ptr(), WIDTH,
              HEIGHT, DISPARITIES, self.costs.data_ptr(), s)
-        if paths_events:
-            paths_events[0].record()
+        mark(3)
         call("nxs_paths_device", self.costs.data_ptr(), WIDTH, HEIGHT, DISPARITIES, PATHS, 8, 64,
              self.volumes.data_ptr(), s)
-        if paths_events:
-            paths_events[1].record()
+        mark(4)
         call("nxs_select_paths_device", self.volumes.data_ptr(), WIDTH, HEIGHT, DISPARITIES,
              PATHS, 1.0526315789473684, self.selected.data_ptr(), self.keys.data_ptr(), s)
+        mark(5)
         call("nxs_consistency_device", self.selected.data_ptr(), self.keys.data_ptr(), WIDTH,
              HEIGHT, self.checked.data_ptr(), s)
+        mark(6)
         call("nxs_median3_device", self.checked.data_ptr(), WIDTH, HEIGHT, 1,
              self.disparity.data_ptr(), s)
+        mark(7)
         call("nxs_despeckle_device", self.disparity.data_ptr(), WIDTH, HEIGHT, 12.0, 1.0, 3,
              self.speckled.data_ptr(), s)
+        mark(8)
         call("nxs_depth_device", self.speckled.data_ptr(), WIDTH * HEIGHT, self.focal,
              self.baseline, self.depth_mm.data_ptr(), self.depth_m.data_ptr(), s)
+        mark(9)
         call("nxs_cloud_device", self.depth_m.data_ptr(), WIDTH, HEIGHT, DECIMATION, self.focal,
              self.cx, self.cy, 0.05, 20.0, self.grid.data_ptr(), self.kept.data_ptr(), s)
+        mark(10)
 
 
 def run_ours(args, rank, world, local_rank):
@@ -218,21 +234,20 @@ def run_ours(args, rank, world, local_rank):
         sampler = ClockSampler(local_rank if os.environ.get("CUDA_VISIBLE_DEVICES") is None else None)
         sampler.start()
         time.sleep(0.3)
-        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        paths_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-                    for _ in range(args.steps)]
+        n_marks = len(DevicePipeline.STAGES) + 1
+        marks = [[torch.cuda.Event(enable_timing=True) for _ in range(n_marks)]
+                 for _ in range(args.steps)]
         torch.cuda.synchronize()
         t0 = time.monotonic()
         for i in range(args.steps):
             flush.fill_(i & 0xFF)  # evict L2 between timed steps, outside the events
-            starts[i].record()
-            pipe.step(d_frames[i % len(d_frames)], paths_ev[i])
-            ends[i].record()
+            pipe.step(d_frames[i % len(d_frames)], marks[i])
         torch.cuda.synchronize()
         t1 = time.monotonic()
-        step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
-        paths_ms = [a.elapsed_time(b) for a, b in paths_ev]
+        step_ms = [m[0].elapsed_time(m[-1]) for m in marks]
+        stage_ms = {name: statistics.mean(m[k].elapsed_time(m[k + 1]) for m in marks)
+                    for k, name in enumerate(DevicePipeline.STAGES)}
+        paths_ms = [m[3].elapsed_time(m[4]) for m in marks]
     total_s = sum(step_ms) / 1000.0
     if dist:
         t = torch.tensor([total_s], device="cuda", dtype=torch.float64)
@@ -311,6 +326,7 @@ def run_ours(args, rank, world, local_rank):
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": paths_bytes,
                      "avg_launch_ms": round(paths_avg_s * 1000, 4), "traffic": None},
+        "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "pipeline_roofline": {"b_alg_per_pair": b_alg,
                               "achieved_gbs": round(b_alg * value / world / 1e9, 1),
                               "frac": round(b_alg * value / world / 1e9 / peak, 4)},

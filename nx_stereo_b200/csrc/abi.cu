@@ -397,8 +397,8 @@ extern "C" nxs_status nxs_select_paths_device(const uint8_t *d_paths, uint32_t w
 extern "C" nxs_status nxs_select_device(const uint16_t *d_sums, uint32_t width, uint32_t height,
                                         uint32_t disparities, float uniqueness,
                                         float *d_disparity, uint32_t *d_keys, void *stream) {
-    CHECK_SIZE(d_sums && d_disparity && d_keys && width > 0 && height > 0 && disparities >= 4 &&
-               disparities <= 256 && disparities % 8 == 0);
+    CHECK_SIZE(d_sums && d_disparity && d_keys && width > 0 && height > 0 && disparities >= 16 &&
+               disparities <= 256 && disparities % 16 == 0);
     return launch_select_sums(d_sums, width, height, disparities, uniqueness, d_disparity, d_keys,
                               static_cast<cudaStream_t>(stream))
                ? NXS_CUDA_ERROR

@@ -72,157 +72,172 @@ cudaError_t launch_census(const uint8_t *left, const uint8_t *right, int width, 
 // ---------------------------------------------------------------- costs
 // costs[y][x][d] = popcount(left[y][x] ^ right[y][x - d]), right codes left of
 // the image zero (lib/nx_stereo.ex:528-542). A block covers 32 pixels of a
-// row; it stages their left codes and the D + 31 right codes they reach, then
-// writes the block's 32 x D bytes with 16-byte stores.
+// row. It stages their left codes and the D + 31 right codes they reach; a
+// warp computes 16 disparities of 32 consecutive pixels (consecutive shared
+// memory words, no bank conflicts) into a shared tile, and the block then
+// writes its 32 x D bytes out contiguously with 16-byte stores.
 constexpr int kCostPixels = 32;
 
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(256)
     costs_kernel(const uint64_t *__restrict__ left_codes, const uint64_t *__restrict__ right_codes,
                  int width, int disparities, uint8_t *__restrict__ costs) {
-    extern __shared__ uint64_t staged[];
-    uint64_t *lefts = staged;
-    uint64_t *rights = staged + kCostPixels;
+    extern __shared__ __align__(16) uint8_t staged[];
+    const int D = disparities, pitch = D + 16;  // tile row pitch: 16-byte stores spread banks
+    uint64_t *lefts = reinterpret_cast<uint64_t *>(staged);
+    uint64_t *rights = lefts + kCostPixels;
+    uint8_t *tile = staged + sizeof(uint64_t) * (2 * kCostPixels + D);
     const int x0 = blockIdx.x * kCostPixels, y = blockIdx.y;
     const size_t row = (size_t)y * width;
     for (int i = threadIdx.x; i < kCostPixels; i += blockDim.x)
         lefts[i] = x0 + i < width ? left_codes[row + x0 + i] : 0;
-    for (int i = threadIdx.x; i < kCostPixels + disparities - 1; i += blockDim.x) {
-        int x = x0 - (disparities - 1) + i;
+    for (int i = threadIdx.x; i < kCostPixels + D - 1; i += blockDim.x) {
+        const int x = x0 - (D - 1) + i;
         rights[i] = (x >= 0 && x < width) ? right_codes[row + x] : 0;
     }
     __syncthreads();
-    const int pixels = min(kCostPixels, width - x0);
-    const int chunks = disparities / 16;
-    for (int c = threadIdx.x; c < pixels * chunks; c += blockDim.x) {
-        const int p = c / chunks, d0 = (c % chunks) * 16;
+    const int chunks = D / 16;
+    for (int t = threadIdx.x; t < kCostPixels * chunks; t += blockDim.x) {
+        const int p = t % kCostPixels, d0 = (t / kCostPixels) * 16;
         const uint64_t l = lefts[p];
         // right code of pixel x0 + p at disparity d: rights[p - d + D - 1]
-        const uint64_t *r = rights + p + disparities - 1 - d0;
+        const uint64_t *r = rights + p + D - 1 - d0;
         uint32_t words[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            uint32_t b0 = __popcll(l ^ r[-(4 * q + 0)]);
-            uint32_t b1 = __popcll(l ^ r[-(4 * q + 1)]);
-            uint32_t b2 = __popcll(l ^ r[-(4 * q + 2)]);
-            uint32_t b3 = __popcll(l ^ r[-(4 * q + 3)]);
+            const uint32_t b0 = __popcll(l ^ r[-(4 * q + 0)]);
+            const uint32_t b1 = __popcll(l ^ r[-(4 * q + 1)]);
+            const uint32_t b2 = __popcll(l ^ r[-(4 * q + 2)]);
+            const uint32_t b3 = __popcll(l ^ r[-(4 * q + 3)]);
             words[q] = b0 | (b1 << 8) | (b2 << 16) | (b3 << 24);
         }
-        *reinterpret_cast<uint4 *>(costs + (row + x0 + p) * disparities + d0) =
+        *reinterpret_cast<uint4 *>(tile + p * pitch + d0) =
             make_uint4(words[0], words[1], words[2], words[3]);
     }
+    __syncthreads();
+    const int pixels = min(kCostPixels, width - x0);
+    uint4 *out = reinterpret_cast<uint4 *>(costs + (row + x0) * D);
+    for (int c = threadIdx.x; c < pixels * chunks; c += blockDim.x)
+        out[c] = *reinterpret_cast<const uint4 *>(tile + (c / chunks) * pitch + (c % chunks) * 16);
 }
 
 cudaError_t launch_costs(const uint64_t *left_codes, const uint64_t *right_codes, int width,
                          int height, int disparities, uint8_t *costs, cudaStream_t stream) {
     dim3 grid((width + kCostPixels - 1) / kCostPixels, height);
-    size_t shared = sizeof(uint64_t) * (2 * kCostPixels + disparities - 1);
-    costs_kernel<<<grid, 128, shared, stream>>>(left_codes, right_codes, width, disparities,
+    const size_t shared = sizeof(uint64_t) * (2 * kCostPixels + disparities) +
+                          (size_t)kCostPixels * (disparities + 16);
+    costs_kernel<<<grid, 256, shared, stream>>>(left_codes, right_codes, width, disparities,
                                                 costs);
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- paths
 // libSGM's normalised recurrence (lib/nx_stereo.ex:575-606) along every scan
-// line of every direction, one warp per line. Lane l holds disparities
-// l*DPL .. l*DPL + DPL - 1 as u16x2 words, unnormalised:
+// line of every direction. A group of G lanes follows one line, each lane
+// holding 16 disparities as eight u16x2 words, so a warp follows 32 / G lines
+// in lockstep (G = 8 at D = 128: four lines per warp). Unnormalised:
 //   L[d] = min(prev[d], prev[d-1] + p1, prev[d+1] + p1, m + p2) - m + C[d],
 //   m = min over d of prev,
 // which equals the reference's min(min(a, p2), min(a[d-1], a[d+1]) + p1) + C
 // with a = prev - m; its out-of-range neighbours (p2 - p1, so p2 once p1 is
-// added) never beat m + p2, so they read as +inf here. Lanes past D hold +inf.
+// added) never beat m + p2, so they read as +inf. Lanes past D hold +inf.
 // A path starts from zero where it enters the image, so its first step is C.
-// The costs of the next kPrefetch steps are in flight while a step computes.
-constexpr int kPrefetch = 4;
+// Each lane moves 16 bytes per step (one copy of costs, one store of path
+// costs); the costs of the next kPrefetch - 1 steps are in flight while a
+// step computes.
+constexpr int kPrefetch = 8;
 
 struct PathSetup {
     int width, height, disparities, p1, p2, paths;
     int first_warp[9];  // first warp of each direction; first_warp[paths] = total
+    int lines[8];       // scan lines of each direction
     int dy[8], dx[8];
     size_t volume;      // bytes of one direction's volume
 };
 
-template <int DPL>
-struct Chunk;
-template <>
-struct Chunk<2> {
-    using T = uint16_t;
-    static __device__ __forceinline__ void unpack(T c, uint32_t *w) {
-        w[0] = __byte_perm((uint32_t)c, 0, 0x4140);
-    }
-    static __device__ __forceinline__ T pack(const uint32_t *w) {
-        return (T)__byte_perm(w[0], 0, 0x4420);
-    }
-    static __device__ __forceinline__ T zero() { return 0; }
-};
-template <>
-struct Chunk<4> {
-    using T = uint32_t;
-    static __device__ __forceinline__ void unpack(T c, uint32_t *w) {
-        w[0] = __byte_perm(c, 0, 0x4140);
-        w[1] = __byte_perm(c, 0, 0x4342);
-    }
-    static __device__ __forceinline__ T pack(const uint32_t *w) {
-        return __byte_perm(w[0], w[1], 0x6420);
-    }
-    static __device__ __forceinline__ T zero() { return 0; }
-};
-template <>
-struct Chunk<8> {
-    using T = uint2;
-    static __device__ __forceinline__ void unpack(T c, uint32_t *w) {
-        w[0] = __byte_perm(c.x, 0, 0x4140);
-        w[1] = __byte_perm(c.x, 0, 0x4342);
-        w[2] = __byte_perm(c.y, 0, 0x4140);
-        w[3] = __byte_perm(c.y, 0, 0x4342);
-    }
-    static __device__ __forceinline__ T pack(const uint32_t *w) {
-        return make_uint2(__byte_perm(w[0], w[1], 0x6420), __byte_perm(w[2], w[3], 0x6420));
-    }
-    static __device__ __forceinline__ T zero() { return make_uint2(0, 0); }
-};
+__device__ __forceinline__ void unpack16(const uint4 c, uint32_t *w) {
+    w[0] = __byte_perm(c.x, 0, 0x4140);
+    w[1] = __byte_perm(c.x, 0, 0x4342);
+    w[2] = __byte_perm(c.y, 0, 0x4140);
+    w[3] = __byte_perm(c.y, 0, 0x4342);
+    w[4] = __byte_perm(c.z, 0, 0x4140);
+    w[5] = __byte_perm(c.z, 0, 0x4342);
+    w[6] = __byte_perm(c.w, 0, 0x4140);
+    w[7] = __byte_perm(c.w, 0, 0x4342);
+}
 
-template <int DPL>
+__device__ __forceinline__ uint4 pack16(const uint32_t *w) {
+    return make_uint4(__byte_perm(w[0], w[1], 0x6420), __byte_perm(w[2], w[3], 0x6420),
+                      __byte_perm(w[4], w[5], 0x6420), __byte_perm(w[6], w[7], 0x6420));
+}
+
+// The start and length of scan line `line` of direction (dy, dx): rows run
+// along x, columns along y, and a diagonal enters from the first row it meets
+// (line < W) or from the side column it meets.
+__device__ __forceinline__ int line_start(int line, int dy, int dx, int W, int H, int *y0,
+                                          int *x0) {
+    if (dy == 0) {
+        *y0 = line;
+        *x0 = dx > 0 ? 0 : W - 1;
+        return W;
+    }
+    if (dx == 0) {
+        *x0 = line;
+        *y0 = dy > 0 ? 0 : H - 1;
+        return H;
+    }
+    if (line < W) {
+        *x0 = line;
+        *y0 = dy > 0 ? 0 : H - 1;
+    } else {
+        *x0 = dx > 0 ? 0 : W - 1;
+        const int k = line - W + 1;
+        *y0 = dy > 0 ? k : H - 1 - k;
+    }
+    const int rows = dy > 0 ? H - *y0 : *y0 + 1;
+    const int columns = dx > 0 ? W - *x0 : *x0 + 1;
+    return min(rows, columns);
+}
+
+// 16-byte global -> shared copies that complete asynchronously (cp.async):
+// the next kStages - 1 steps' costs are in flight while a step computes, and
+// a thread reads back only the slots it filled. src_size 0 zero-fills.
+__device__ __forceinline__ void copy16_async(void *shared, const void *global, bool valid) {
+    const unsigned address = (unsigned)__cvta_generic_to_shared(shared);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(address), "l"(global),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void copy_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void copy_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <int G, bool FULL>
 __global__ void __launch_bounds__(128)
     paths_kernel(const uint8_t *__restrict__ costs, uint8_t *__restrict__ paths_out,
                  const PathSetup s) {
-    using C = Chunk<DPL>;
-    using T = typename C::T;
-    constexpr int R = DPL / 2;  // u16x2 words per lane
+    constexpr int R = 8;            // u16x2 words per lane: 16 disparities
+    constexpr int LINES = 32 / G;   // lines per warp
+    __shared__ uint4 ring[kPrefetch][128];
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= s.first_warp[s.paths]) return;  // the whole warp leaves together
     int p = 0;
     while (warp >= s.first_warp[p + 1]) ++p;
-    const int line = warp - s.first_warp[p];
+    const int group = lane / G, member = lane % G;
+    const int line = (warp - s.first_warp[p]) * LINES + group;
     const int dy = s.dy[p], dx = s.dx[p];
-    const int W = s.width, H = s.height;
-    int y0, x0, length;
-    if (dy == 0) {  // along a row
-        y0 = line;
-        x0 = dx > 0 ? 0 : W - 1;
-        length = W;
-    } else if (dx == 0) {  // down or up a column
-        x0 = line;
-        y0 = dy > 0 ? 0 : H - 1;
-        length = H;
-    } else {  // a diagonal, entering from the first row it meets or from a side
-        if (line < W) {
-            x0 = line;
-            y0 = dy > 0 ? 0 : H - 1;
-        } else {
-            x0 = dx > 0 ? 0 : W - 1;
-            int k = line - W + 1;
-            y0 = dy > 0 ? k : H - 1 - k;
-        }
-        int rows = dy > 0 ? H - y0 : y0 + 1;
-        int columns = dx > 0 ? W - x0 : x0 + 1;
-        length = min(rows, columns);
-    }
-    const int D = s.disparities;
-    const bool active = lane * DPL < D;
+    const int W = s.width, H = s.height, D = s.disparities;
+    int y0 = 0, x0 = 0, length = 0;
+    if (line < s.lines[p]) length = line_start(line, dy, dx, W, H, &y0, &x0);
+    const bool active = FULL || member * 16 < D;
     const ptrdiff_t stride = ((ptrdiff_t)dy * W + dx) * D;
-    const uint8_t *src = costs + ((size_t)y0 * W + x0) * D + lane * DPL;
-    uint8_t *dst = paths_out + (size_t)p * s.volume + ((size_t)y0 * W + x0) * D + lane * DPL;
+    const size_t at = ((size_t)y0 * W + x0) * D + member * 16;
+    const uint8_t *ahead = costs + at;
+    uint8_t *dst = paths_out + (size_t)p * s.volume + at;
+    const int steps = (int)__reduce_max_sync(kFullMask, (unsigned)length);
+    uint4 *slot = &ring[0][threadIdx.x];
 
     uint32_t r[R];
 #pragma unroll
@@ -230,56 +245,64 @@ __global__ void __launch_bounds__(128)
     uint32_t m2 = 0, j2 = (uint32_t)s.p2 * 0x10001u;
     const uint32_t p1x2 = (uint32_t)s.p1 * 0x10001u;
 
-    T ring[kPrefetch];
 #pragma unroll
-    for (int i = 0; i < kPrefetch; ++i)
-        ring[i] = (active && i < length) ? __ldg(reinterpret_cast<const T *>(src + i * stride))
-                                         : C::zero();
-
-    for (int base = 0; base < length; base += kPrefetch) {
+    for (int i = 0; i < kPrefetch - 1; ++i) {
+        const bool valid = active && i < length;
+        copy16_async(slot + i * 128, valid ? ahead : costs, valid);
+        copy_commit();
+        ahead += stride;
+    }
+    for (int base = 0; base < steps; base += kPrefetch) {
 #pragma unroll
         for (int i = 0; i < kPrefetch; ++i) {
             const int step = base + i;
-            if (step >= length) break;  // uniform across the warp
-            const T c = ring[i];
-            const int ahead = step + kPrefetch;
-            ring[i] = (active && ahead < length)
-                          ? __ldg(reinterpret_cast<const T *>(src + ahead * stride))
-                          : C::zero();
+            if (step >= steps) break;  // uniform across the warp
+            {   // the copy of step + kPrefetch - 1 goes to the slot read last step
+                const bool valid = active && step + kPrefetch - 1 < length;
+                copy16_async(slot + ((i + kPrefetch - 1) % kPrefetch) * 128,
+                             valid ? ahead : costs, valid);
+                copy_commit();
+                ahead += stride;
+            }
+            copy_wait<kPrefetch - 1>();
             uint32_t cost[R];
-            C::unpack(c, cost);
+            unpack16(slot[i * 128], cost);
             uint32_t from_left = __shfl_up_sync(kFullMask, r[R - 1], 1);
             uint32_t from_right = __shfl_down_sync(kFullMask, r[0], 1);
-            if (lane == 0) from_left = kInf2;
-            if (lane == 31) from_right = kInf2;
-            uint32_t shifted[R + 1];  // shifted[k] = (d-1) values of word k
+            if (member == 0) from_left = kInf2;
+            if (member == G - 1) from_right = kInf2;
+            uint32_t shifted[R + 1];  // shifted[k]: the (d - 1) values of word k
             shifted[0] = __byte_perm(from_left, r[0], 0x5432);
 #pragma unroll
             for (int k = 1; k < R; ++k) shifted[k] = __byte_perm(r[k - 1], r[k], 0x5432);
             shifted[R] = __byte_perm(r[R - 1], from_right, 0x5432);
-            uint32_t lowest = kInf2;
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                uint32_t neighbour = vmin2(shifted[k], shifted[k + 1]);
+                const uint32_t neighbour = vmin2(shifted[k], shifted[k + 1]);
                 uint32_t t = vmin2(r[k], j2);
                 t = __viaddmin_u16x2(neighbour, p1x2, t);
                 // t >= m in both halves, so the subtraction borrows nowhere.
-                uint32_t value = t - m2 + cost[k];
-                r[k] = active ? value : kInf2;
-                lowest = vmin2(lowest, r[k]);
+                const uint32_t value = t - m2 + cost[k];
+                r[k] = (FULL || active) ? value : kInf2;
             }
-            if (active) *reinterpret_cast<T *>(dst + step * stride) = C::pack(r);
+            if (active && step < length) *reinterpret_cast<uint4 *>(dst) = pack16(r);
+            dst += stride;
+            const uint32_t lowest = vmin2(__vimin3_u16x2(r[0], r[1], r[2]),
+                                          __vimin3_u16x2(__vimin3_u16x2(r[3], r[4], r[5]), r[6], r[7]));
             uint32_t m = min(lowest & 0xFFFFu, lowest >> 16);
-            m = __reduce_min_sync(kFullMask, m);
+#pragma unroll
+            for (int offset = G / 2; offset >= 1; offset /= 2)
+                m = min(m, __shfl_xor_sync(kFullMask, m, offset));
             m2 = m * 0x10001u;
             j2 = (m + (uint32_t)s.p2) * 0x10001u;
         }
     }
+    copy_wait<0>();
 }
 
-static int lanes_disparities(int disparities) {
-    // Disparities per lane: a warp of 32 lanes covers up to 32 * DPL.
-    return disparities <= 64 ? 2 : (disparities <= 128 ? 4 : 8);
+static int group_lanes(int disparities) {
+    // Lanes per scan line, 16 disparities each, a power of two.
+    return disparities <= 64 ? 4 : (disparities <= 128 ? 8 : 16);
 }
 
 cudaError_t launch_paths(const uint8_t *costs, int width, int height, int disparities, int paths,
@@ -292,21 +315,24 @@ cudaError_t launch_paths(const uint8_t *costs, int width, int height, int dispar
     s.p2 = p2;
     s.paths = paths;
     s.volume = (size_t)width * height * disparities;
+    const int g = group_lanes(disparities), lines_per_warp = 32 / g;
+    const bool full = g * 16 == disparities;
     int total = 0;
     for (int p = 0; p < paths; ++p) {
         s.first_warp[p] = total;
         s.dy[p] = kDirections[p][0];
         s.dx[p] = kDirections[p][1];
-        total += s.dy[p] == 0 ? height : (s.dx[p] == 0 ? width : width + height - 1);
+        s.lines[p] = s.dy[p] == 0 ? height : (s.dx[p] == 0 ? width : width + height - 1);
+        total += (s.lines[p] + lines_per_warp - 1) / lines_per_warp;
     }
     s.first_warp[paths] = total;
     const int threads = 128, warps_per_block = threads / 32;
     const int blocks = (total + warps_per_block - 1) / warps_per_block;
-    switch (lanes_disparities(disparities)) {
-    case 2: paths_kernel<2><<<blocks, threads, 0, stream>>>(costs, paths_out, s); break;
-    case 4: paths_kernel<4><<<blocks, threads, 0, stream>>>(costs, paths_out, s); break;
-    default: paths_kernel<8><<<blocks, threads, 0, stream>>>(costs, paths_out, s); break;
-    }
+#define NXS_PATHS(G, F) paths_kernel<G, F><<<blocks, threads, 0, stream>>>(costs, paths_out, s)
+    if (g == 4) full ? NXS_PATHS(4, true) : NXS_PATHS(4, false);
+    else if (g == 8) full ? NXS_PATHS(8, true) : NXS_PATHS(8, false);
+    else full ? NXS_PATHS(16, true) : NXS_PATHS(16, false);
+#undef NXS_PATHS
     return cudaGetLastError();
 }
 
@@ -335,76 +361,94 @@ cudaError_t launch_sum_paths(const uint8_t *paths_in, int width, int height, int
 }
 
 // ---------------------------------------------------------------- select
-// Winner, uniqueness and subpixel (lib/nx_stereo.ex:608-641), one warp per
-// pixel, lanes over disparities. values = sums + 0x8000 past x; the winner is
-// the lowest (value << 16 | d), so ties go to the lowest d; `second` is the
+// Winner, uniqueness and subpixel (lib/nx_stereo.ex:608-641). A group of G
+// lanes takes one pixel, each lane 16 disparities, so a warp takes 32 / G
+// pixels. values = sum of the path costs + 0x8000 past x; the winner is the
+// lowest (value << 16 | d), so ties go to the lowest d; `second` is the
 // lowest value more than one disparity from the winner; the f32 steps are
-// rounded one at a time in the reference's order.
-template <int DPL, bool FROM_SUMS>
+// rounded one at a time in the reference's order. Two path volumes add as
+// bytes without carry (127 + 127 < 256) before widening to u16x2.
+template <int G, bool FROM_SUMS>
 __global__ void __launch_bounds__(128)
     select_kernel(const void *__restrict__ source, int width, int height, int disparities,
                   int paths, size_t volume, float uniqueness, float *__restrict__ disparity,
                   uint32_t *__restrict__ keys) {
-    const size_t pixel = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    constexpr int PIXELS = 128 / G;  // per block
+    __shared__ __align__(16) uint16_t values_of[PIXELS][256];
     const int lane = threadIdx.x & 31;
-    if (pixel >= (size_t)width * height) return;
-    const int x = (int)(pixel % width);
+    const int slot = threadIdx.x / G, member = threadIdx.x % G;
+    const size_t pixel = (size_t)blockIdx.x * PIXELS + slot;
+    const bool valid = pixel < (size_t)width * height;
     const int D = disparities;
-    const bool active = lane * DPL < D;
-    uint32_t sum[DPL];
+    const bool active = valid && member * 16 < D;
+    const int x = valid ? (int)(pixel % width) : 0;
+    const int d0 = member * 16;
+    uint32_t v[8];
 #pragma unroll
-    for (int i = 0; i < DPL; ++i) sum[i] = 0;
+    for (int k = 0; k < 8; ++k) v[k] = 0;
     if (active) {
-        const size_t at = pixel * D + lane * DPL;
+        const size_t at = pixel * D + d0;
         if (FROM_SUMS) {
-            const uint16_t *sums = static_cast<const uint16_t *>(source) + at;
-#pragma unroll
-            for (int i = 0; i < DPL; ++i) sum[i] = sums[i];
+            const uint4 *sums = reinterpret_cast<const uint4 *>(static_cast<const uint16_t *>(source) + at);
+            const uint4 a = sums[0], b = sums[1];
+            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+            v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
         } else {
             const uint8_t *volumes = static_cast<const uint8_t *>(source) + at;
-            uint32_t packed[DPL / 2];
+            int p = 0;
+            for (; p + 1 < paths; p += 2) {
+                const uint4 a = __ldg(reinterpret_cast<const uint4 *>(volumes + p * volume));
+                const uint4 b = __ldg(reinterpret_cast<const uint4 *>(volumes + (p + 1) * volume));
+                uint32_t pair[8];
+                unpack16(make_uint4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w), pair);
 #pragma unroll
-            for (int k = 0; k < DPL / 2; ++k) packed[k] = 0;
-            for (int p = 0; p < paths; ++p) {
-                uint32_t words[DPL / 2];
-                Chunk<DPL>::unpack(
-                    __ldg(reinterpret_cast<const typename Chunk<DPL>::T *>(volumes + p * volume)),
-                    words);
-#pragma unroll
-                for (int k = 0; k < DPL / 2; ++k) packed[k] += words[k];
+                for (int k = 0; k < 8; ++k) v[k] += pair[k];
             }
+            if (p < paths) {
+                uint32_t single[8];
+                unpack16(__ldg(reinterpret_cast<const uint4 *>(volumes + p * volume)), single);
 #pragma unroll
-            for (int k = 0; k < DPL / 2; ++k) {
-                sum[2 * k] = packed[k] & 0xFFFFu;
-                sum[2 * k + 1] = packed[k] >> 16;
+                for (int k = 0; k < 8; ++k) v[k] += single[k];
             }
         }
-    }
-    uint32_t value[DPL];
-    uint32_t best = 0xFFFFFFFFu;
+        if (x < d0 + 15) {  // disparities past the left edge lose
 #pragma unroll
-    for (int i = 0; i < DPL; ++i) {
-        const int d = lane * DPL + i;
-        value[i] = sum[i] + (d > x ? 0x8000u : 0u);
-        if (active) best = min(best, (value[i] << 16) | (uint32_t)d);
+            for (int k = 0; k < 8; ++k)
+                v[k] += (d0 + 2 * k > x ? 0x8000u : 0u) | (d0 + 2 * k + 1 > x ? 0x80000000u : 0u);
+        }
+        *reinterpret_cast<uint4 *>(&values_of[slot][d0]) = make_uint4(v[0], v[1], v[2], v[3]);
+        *reinterpret_cast<uint4 *>(&values_of[slot][d0 + 8]) = make_uint4(v[4], v[5], v[6], v[7]);
     }
-    best = __reduce_min_sync(kFullMask, best);
+    uint32_t best = 0xFFFFFFFFu;
+    if (active) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t d = (uint32_t)(d0 + 2 * k) | ((uint32_t)(d0 + 2 * k + 1) << 16);
+            best = min(best, min(__byte_perm(v[k], d, 0x1054), __byte_perm(v[k], d, 0x3276)));
+        }
+    }
+#pragma unroll
+    for (int offset = G / 2; offset >= 1; offset /= 2)
+        best = min(best, __shfl_xor_sync(kFullMask, best, offset));
     const uint32_t minimum = best >> 16;
     const int winner = (int)(best & 0xFFFFu);
-    const int below = max(winner - 1, 0), above = min(winner + 1, D - 1);
-    uint32_t second = 0xFFFFFFFFu, lower = 0xFFFFFFFFu, upper = 0xFFFFFFFFu;
+    uint32_t second = 0xFFFFFFFFu;
+    if (active) {
 #pragma unroll
-    for (int i = 0; i < DPL; ++i) {
-        const int d = lane * DPL + i;
-        if (!active) continue;
-        if (d < winner - 1 || d > winner + 1) second = min(second, value[i]);
-        if (d == below) lower = value[i];
-        if (d == above) upper = value[i];
+        for (int k = 0; k < 8; ++k) {
+            const int d = d0 + 2 * k;
+            // d outside [winner - 1, winner + 1]
+            if ((unsigned)(d - winner + 1) > 2u) second = min(second, v[k] & 0xFFFFu);
+            if ((unsigned)(d + 1 - winner + 1) > 2u) second = min(second, v[k] >> 16);
+        }
     }
-    second = __reduce_min_sync(kFullMask, second);
-    lower = __reduce_min_sync(kFullMask, lower);
-    upper = __reduce_min_sync(kFullMask, upper);
-    if (lane != 0) return;
+#pragma unroll
+    for (int offset = G / 2; offset >= 1; offset /= 2)
+        second = min(second, __shfl_xor_sync(kFullMask, second, offset));
+    __syncwarp();
+    if (member != 0 || !valid) return;
+    const uint32_t lower = values_of[slot][max(winner - 1, 0)];
+    const uint32_t upper = values_of[slot][min(winner + 1, D - 1)];
     const float lower_f = (float)lower, upper_f = (float)upper, minimum_f = (float)minimum;
     // With no disparity outside the winner's neighbours the reference's
     // minimum is i32::MAX (lib/nx_stereo.ex:620-622).
@@ -426,21 +470,16 @@ static cudaError_t launch_select(const void *source, int width, int height, int 
                                  cudaStream_t stream) {
     const size_t pixels = (size_t)width * height;
     const size_t volume = pixels * disparities;
-    const unsigned blocks = (unsigned)((pixels * 32 + 127) / 128);
-    switch (lanes_disparities(disparities)) {
-    case 2:
-        select_kernel<2, FROM_SUMS><<<blocks, 128, 0, stream>>>(
-            source, width, height, disparities, paths, volume, uniqueness, disparity, keys);
-        break;
-    case 4:
-        select_kernel<4, FROM_SUMS><<<blocks, 128, 0, stream>>>(
-            source, width, height, disparities, paths, volume, uniqueness, disparity, keys);
-        break;
-    default:
-        select_kernel<8, FROM_SUMS><<<blocks, 128, 0, stream>>>(
-            source, width, height, disparities, paths, volume, uniqueness, disparity, keys);
-        break;
-    }
+    const int g = group_lanes(disparities);
+    const unsigned blocks = (unsigned)((pixels + 128 / g - 1) / (128 / g));
+#define NXS_SELECT(G)                                                                  \
+    select_kernel<G, FROM_SUMS><<<blocks, 128, 0, stream>>>(source, width, height,      \
+                                                             disparities, paths, volume, \
+                                                             uniqueness, disparity, keys)
+    if (g == 4) NXS_SELECT(4);
+    else if (g == 8) NXS_SELECT(8);
+    else NXS_SELECT(16);
+#undef NXS_SELECT
     return cudaGetLastError();
 }
 
