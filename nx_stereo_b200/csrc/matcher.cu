@@ -132,18 +132,19 @@ cudaError_t launch_costs(const uint64_t *left_codes, const uint64_t *right_codes
 
 // ---------------------------------------------------------------- paths
 // libSGM's normalised recurrence (lib/nx_stereo.ex:575-606) along every scan
-// line of every direction. A group of G lanes follows one line, each lane
-// holding 16 disparities as eight u16x2 words, so a warp follows 32 / G lines
-// in lockstep (G = 8 at D = 128: four lines per warp). Unnormalised:
+// line of every direction, unnormalised:
 //   L[d] = min(prev[d], prev[d-1] + p1, prev[d+1] + p1, m + p2) - m + C[d],
 //   m = min over d of prev,
 // which equals the reference's min(min(a, p2), min(a[d-1], a[d+1]) + p1) + C
 // with a = prev - m; its out-of-range neighbours (p2 - p1, so p2 once p1 is
 // added) never beat m + p2, so they read as +inf. Lanes past D hold +inf.
 // A path starts from zero where it enters the image, so its first step is C.
-// Each lane moves 16 bytes per step (one copy of costs, one store of path
-// costs); the costs of the next kPrefetch - 1 steps are in flight while a
-// step computes.
+//
+// A group of G lanes follows one line, each lane holding 2 * WORDS
+// disparities as u16x2 words (five integer instructions per word and step),
+// and a warp follows 32 / G lines in lockstep. Each lane copies its costs for the next kPrefetch - 1 steps into a shared
+// ring with cp.async while a step computes, and stores its path costs with
+// 16-byte stores.
 constexpr int kPrefetch = 8;
 
 struct PathSetup {
@@ -151,6 +152,8 @@ struct PathSetup {
     int first_warp[9];  // first warp of each direction; first_warp[paths] = total
     int lines[8];       // scan lines of each direction
     int dy[8], dx[8];
+    int order[8];       // direction of each slot: rows first, then columns, then diagonals
+    int straight;       // slots of rows and columns
     size_t volume;      // bytes of one direction's volume
 };
 
@@ -198,9 +201,8 @@ __device__ __forceinline__ int line_start(int line, int dy, int dx, int W, int H
     return min(rows, columns);
 }
 
-// 16-byte global -> shared copies that complete asynchronously (cp.async):
-// the next kStages - 1 steps' costs are in flight while a step computes, and
-// a thread reads back only the slots it filled. src_size 0 zero-fills.
+// 16-byte global -> shared copies that complete asynchronously (cp.async);
+// src_size 0 zero-fills without reading.
 __device__ __forceinline__ void copy16_async(void *shared, const void *global, bool valid) {
     const unsigned address = (unsigned)__cvta_generic_to_shared(shared);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(address), "l"(global),
@@ -213,42 +215,37 @@ __device__ __forceinline__ void copy_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-template <int G, bool FULL>
-__global__ void __launch_bounds__(128)
-    paths_kernel(const uint8_t *__restrict__ costs, uint8_t *__restrict__ paths_out,
-                 const PathSetup s) {
-    constexpr int R = 8;            // u16x2 words per lane: 16 disparities
-    constexpr int LINES = 32 / G;   // lines per warp
-    __shared__ uint4 ring[kPrefetch][128];
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= s.first_warp[s.paths]) return;  // the whole warp leaves together
-    int p = 0;
-    while (warp >= s.first_warp[p + 1]) ++p;
-    const int group = lane / G, member = lane % G;
-    const int line = (warp - s.first_warp[p]) * LINES + group;
+// The lines of one warp: G lanes per line, WORDS u16x2 words per lane.
+// `ring` is this thread's kPrefetch x (WORDS / 8) slots of 16 bytes, strided
+// by THREADS threads.
+template <int G, int WORDS, bool FULL, int THREADS>
+__device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
+                                             uint8_t *__restrict__ out, const PathSetup &s,
+                                             int p, int line, int member, uint4 *ring) {
+    constexpr int CHUNKS = WORDS / 8;  // 16-byte chunks per lane
     const int dy = s.dy[p], dx = s.dx[p];
     const int W = s.width, H = s.height, D = s.disparities;
     int y0 = 0, x0 = 0, length = 0;
     if (line < s.lines[p]) length = line_start(line, dy, dx, W, H, &y0, &x0);
-    const bool active = FULL || member * 16 < D;
+    const bool active = FULL || member * 2 * WORDS < D;
     const ptrdiff_t stride = ((ptrdiff_t)dy * W + dx) * D;
-    const size_t at = ((size_t)y0 * W + x0) * D + member * 16;
+    const size_t at = ((size_t)y0 * W + x0) * D + member * 2 * WORDS;
     const uint8_t *ahead = costs + at;
-    uint8_t *dst = paths_out + (size_t)p * s.volume + at;
+    uint8_t *dst = out + (size_t)p * s.volume + at;
     const int steps = (int)__reduce_max_sync(kFullMask, (unsigned)length);
-    uint4 *slot = &ring[0][threadIdx.x];
 
-    uint32_t r[R];
+    uint32_t r[WORDS];
 #pragma unroll
-    for (int k = 0; k < R; ++k) r[k] = active ? 0u : kInf2;
+    for (int k = 0; k < WORDS; ++k) r[k] = active ? 0u : kInf2;
     uint32_t m2 = 0, j2 = (uint32_t)s.p2 * 0x10001u;
-    const uint32_t p1x2 = (uint32_t)s.p1 * 0x10001u;
+    const uint32_t p1x2 = (uint32_t)s.p1 * 0x10001u, p2x2 = (uint32_t)s.p2 * 0x10001u;
 
 #pragma unroll
     for (int i = 0; i < kPrefetch - 1; ++i) {
         const bool valid = active && i < length;
-        copy16_async(slot + i * 128, valid ? ahead : costs, valid);
+#pragma unroll
+        for (int c = 0; c < CHUNKS; ++c)
+            copy16_async(ring + (i * CHUNKS + c) * THREADS, valid ? ahead + 16 * c : costs, valid);
         copy_commit();
         ahead += stride;
     }
@@ -259,25 +256,29 @@ __global__ void __launch_bounds__(128)
             if (step >= steps) break;  // uniform across the warp
             {   // the copy of step + kPrefetch - 1 goes to the slot read last step
                 const bool valid = active && step + kPrefetch - 1 < length;
-                copy16_async(slot + ((i + kPrefetch - 1) % kPrefetch) * 128,
-                             valid ? ahead : costs, valid);
+                const int slot = (i + kPrefetch - 1) % kPrefetch;
+#pragma unroll
+                for (int c = 0; c < CHUNKS; ++c)
+                    copy16_async(ring + (slot * CHUNKS + c) * THREADS,
+                                 valid ? ahead + 16 * c : costs, valid);
                 copy_commit();
                 ahead += stride;
             }
             copy_wait<kPrefetch - 1>();
-            uint32_t cost[R];
-            unpack16(slot[i * 128], cost);
-            uint32_t from_left = __shfl_up_sync(kFullMask, r[R - 1], 1);
+            uint32_t cost[WORDS];
+#pragma unroll
+            for (int c = 0; c < CHUNKS; ++c) unpack16(ring[(i * CHUNKS + c) * THREADS], cost + 8 * c);
+            uint32_t from_left = __shfl_up_sync(kFullMask, r[WORDS - 1], 1);
             uint32_t from_right = __shfl_down_sync(kFullMask, r[0], 1);
             if (member == 0) from_left = kInf2;
             if (member == G - 1) from_right = kInf2;
-            uint32_t shifted[R + 1];  // shifted[k]: the (d - 1) values of word k
+            uint32_t shifted[WORDS + 1];  // shifted[k]: the (d - 1) values of word k
             shifted[0] = __byte_perm(from_left, r[0], 0x5432);
 #pragma unroll
-            for (int k = 1; k < R; ++k) shifted[k] = __byte_perm(r[k - 1], r[k], 0x5432);
-            shifted[R] = __byte_perm(r[R - 1], from_right, 0x5432);
+            for (int k = 1; k < WORDS; ++k) shifted[k] = __byte_perm(r[k - 1], r[k], 0x5432);
+            shifted[WORDS] = __byte_perm(r[WORDS - 1], from_right, 0x5432);
 #pragma unroll
-            for (int k = 0; k < R; ++k) {
+            for (int k = 0; k < WORDS; ++k) {
                 const uint32_t neighbour = vmin2(shifted[k], shifted[k + 1]);
                 uint32_t t = vmin2(r[k], j2);
                 t = __viaddmin_u16x2(neighbour, p1x2, t);
@@ -285,24 +286,77 @@ __global__ void __launch_bounds__(128)
                 const uint32_t value = t - m2 + cost[k];
                 r[k] = (FULL || active) ? value : kInf2;
             }
-            if (active && step < length) *reinterpret_cast<uint4 *>(dst) = pack16(r);
+            if (active && step < length) {
+#pragma unroll
+                for (int c = 0; c < CHUNKS; ++c)
+                    *reinterpret_cast<uint4 *>(dst + 16 * c) = pack16(r + 8 * c);
+            }
             dst += stride;
-            const uint32_t lowest = vmin2(__vimin3_u16x2(r[0], r[1], r[2]),
-                                          __vimin3_u16x2(__vimin3_u16x2(r[3], r[4], r[5]), r[6], r[7]));
+            uint32_t lowest = __vimin3_u16x2(r[0], r[1], r[2]);
+#pragma unroll
+            for (int k = 3; k + 1 < WORDS; k += 2) lowest = __vimin3_u16x2(lowest, r[k], r[k + 1]);
+            if (WORDS % 2 == 0) lowest = vmin2(lowest, r[WORDS - 1]);
             uint32_t m = min(lowest & 0xFFFFu, lowest >> 16);
 #pragma unroll
             for (int offset = G / 2; offset >= 1; offset /= 2)
                 m = min(m, __shfl_xor_sync(kFullMask, m, offset));
             m2 = m * 0x10001u;
-            j2 = (m + (uint32_t)s.p2) * 0x10001u;
+            j2 = m2 + p2x2;
         }
     }
     copy_wait<0>();
 }
 
-static int group_lanes(int disparities) {
-    // Lanes per scan line, 16 disparities each, a power of two.
-    return disparities <= 64 ? 4 : (disparities <= 128 ? 8 : 16);
+// The scan line of direction (dy, dx) with rank `rank` when the lines are
+// ordered by length, longest first, so the lines a warp follows together are
+// alike in length. Rows and columns are all alike. A diagonal line either
+// starts on the first row it meets, at a distance j = 1..W from the side it
+// runs away from (length min(H, j)), or on a side column at row offset
+// k = 1..H-1 (length min(H - k, W)).
+__device__ __forceinline__ int ranked_line(int rank, int dy, int dx, int W, int H) {
+    if (dy == 0 || dx == 0) return rank;
+    const int full = (W > H ? W - H : H - W) + 1;  // lines of the greatest length
+    int j = 0, k = 0;                              // first-row distance, or side offset
+    if (rank < full) {
+        if (W >= H) j = W - rank;
+        else if (rank < full - 1) k = rank + 1;
+        else j = W;
+    } else {
+        const int q = rank - full;
+        const int len = min(W, H) - 1 - q / 2;
+        if (q % 2 == 0) j = len;
+        else k = H - len;
+    }
+    if (j > 0) return dx > 0 ? W - j : j - 1;
+    return W - 1 + k;
+}
+
+// G lanes per line, 16 disparities per lane, for every direction. One warp
+// per block, so blocks go to SMs as they free up, longest lines first: rows,
+// then columns, then the diagonals of all four directions by rank.
+template <int G, bool FULL>
+__global__ void __launch_bounds__(32)
+    paths_kernel(const uint8_t *__restrict__ costs, uint8_t *__restrict__ paths_out,
+                 const PathSetup s) {
+    __shared__ uint4 ring[kPrefetch][32];
+    const int warp = blockIdx.x;
+    const int lane = threadIdx.x;
+    int slot = 0;
+    while (warp >= s.first_warp[slot + 1]) ++slot;
+    int p, group;
+    if (slot < s.straight) {  // rows and columns, direction by direction
+        p = s.order[slot];
+        group = warp - s.first_warp[slot];
+    } else {                  // diagonals interleaved, longest first
+        const int w = warp - s.first_warp[s.straight];
+        const int diagonals = s.paths - s.straight;
+        p = s.order[s.straight + w % diagonals];
+        group = w / diagonals;
+    }
+    const int rank = group * (32 / G) + lane / G;
+    const int line =
+        rank < s.lines[p] ? ranked_line(rank, s.dy[p], s.dx[p], s.width, s.height) : rank;
+    follow_lines<G, 8, FULL, 32>(costs, paths_out, s, p, line, lane % G, &ring[0][lane]);
 }
 
 cudaError_t launch_paths(const uint8_t *costs, int width, int height, int disparities, int paths,
@@ -315,25 +369,47 @@ cudaError_t launch_paths(const uint8_t *costs, int width, int height, int dispar
     s.p2 = p2;
     s.paths = paths;
     s.volume = (size_t)width * height * disparities;
-    const int g = group_lanes(disparities), lines_per_warp = 32 / g;
+    // Lanes per line, 16 disparities each: a power of two.
+    const int g = disparities <= 64 ? 4 : (disparities <= 128 ? 8 : 16);
     const bool full = g * 16 == disparities;
-    int total = 0;
+    const int lines_per_warp = 32 / g;
+    // Rows, then columns, then diagonals.
+    int n = 0;
+    for (int pass = 0; pass < 3; ++pass) {
+        for (int p = 0; p < paths; ++p) {
+            const int dy = kDirections[p][0], dx = kDirections[p][1];
+            const int kind = dy == 0 ? 0 : (dx == 0 ? 1 : 2);
+            if (kind == pass) s.order[n++] = p;
+        }
+        if (pass == 1) s.straight = n;
+    }
     for (int p = 0; p < paths; ++p) {
-        s.first_warp[p] = total;
         s.dy[p] = kDirections[p][0];
         s.dx[p] = kDirections[p][1];
         s.lines[p] = s.dy[p] == 0 ? height : (s.dx[p] == 0 ? width : width + height - 1);
-        total += (s.lines[p] + lines_per_warp - 1) / lines_per_warp;
     }
-    s.first_warp[paths] = total;
-    const int threads = 128, warps_per_block = threads / 32;
-    const int blocks = (total + warps_per_block - 1) / warps_per_block;
-#define NXS_PATHS(G, F) paths_kernel<G, F><<<blocks, threads, 0, stream>>>(costs, paths_out, s)
+    int total = 0;
+    for (int slot = 0; slot < s.straight; ++slot) {
+        s.first_warp[slot] = total;
+        total += (s.lines[s.order[slot]] + lines_per_warp - 1) / lines_per_warp;
+    }
+    // The diagonals share one range of warps starting at slot `straight`;
+    // every later slot starts at the end, so the slot search stops in range.
+    const int diagonals = paths - s.straight;
+    s.first_warp[s.straight] = total;
+    if (diagonals) total += (width + height - 1 + lines_per_warp - 1) / lines_per_warp * diagonals;
+    for (int slot = s.straight + 1; slot <= 8; ++slot) s.first_warp[slot] = total;
+#define NXS_PATHS(G, F) paths_kernel<G, F><<<total, 32, 0, stream>>>(costs, paths_out, s)
     if (g == 4) full ? NXS_PATHS(4, true) : NXS_PATHS(4, false);
     else if (g == 8) full ? NXS_PATHS(8, true) : NXS_PATHS(8, false);
     else full ? NXS_PATHS(16, true) : NXS_PATHS(16, false);
 #undef NXS_PATHS
     return cudaGetLastError();
+}
+
+static int group_lanes(int disparities) {
+    // Lanes per pixel in selection, 16 disparities each, a power of two.
+    return disparities <= 64 ? 4 : (disparities <= 128 ? 8 : 16);
 }
 
 // sums[y][x][d] = sum of the P path volumes, u16 (at most 8 x 127 = 1016).
@@ -375,7 +451,6 @@ __global__ void __launch_bounds__(128)
                   uint32_t *__restrict__ keys) {
     constexpr int PIXELS = 128 / G;  // per block
     __shared__ __align__(16) uint16_t values_of[PIXELS][256];
-    const int lane = threadIdx.x & 31;
     const int slot = threadIdx.x / G, member = threadIdx.x % G;
     const size_t pixel = (size_t)blockIdx.x * PIXELS + slot;
     const bool valid = pixel < (size_t)width * height;
