@@ -2,14 +2,15 @@
 // (configure / run / release, the reference Port's three requests) and the
 // direct entry points.
 //
-// A segment owns a CUDA stream, its device buffers and what its stages carry
-// from pair to pair (the temporal filter's previous disparity and missed
-// counts, the quality stage's previous disparity). A request copies its
-// entries into pinned memory, enqueues the host-to-device copies, every
-// member's kernels and the device-to-host copies of the outputs on the
-// segment's stream, and returns; requests on one segment therefore run in
-// the order sent, as the reference's Port computes them
-// (native/stereo_match/src/main.rs:1-11).
+// A segment owns three CUDA streams (upload, compute, download), a ring of
+// per-request device slots and what its stages carry from pair to pair (the
+// temporal filter's previous disparity and missed counts, the quality
+// stage's previous disparity). A request copies its entries into pinned
+// memory, enqueues the upload into its slot, every member's kernels and the
+// download of the outputs, ordered by events, and returns. Compute runs on
+// one stream in request order, as the reference's Port computes them
+// (native/stereo_match/src/main.rs:1-11), while uploads and downloads of
+// neighbouring requests overlap it.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -119,21 +120,37 @@ struct Spec {
     }
 };
 
+// What one request in flight uses on the device: its entries, the outputs it
+// downloads, and the events that order it across the segment's streams.
+struct Slot {
+    uint8_t *frames[2] = {nullptr, nullptr}, *images[2] = {nullptr, nullptr};
+    float *disparity[2] = {nullptr, nullptr}, *grid = nullptr, *quality_sums = nullptr;
+    uint16_t *depth_mm = nullptr;
+    int32_t *kept = nullptr;
+    cudaEvent_t entered = nullptr;   // entries on the device
+    cudaEvent_t computed = nullptr;  // outputs ready
+    cudaEvent_t free = nullptr;      // outputs downloaded: the slot may be reused
+};
+
+// Requests cycle through kSlots slots. Entries go up on `upload`, the members
+// compute on `stream`, outputs come down on `download`: request n + 1's
+// upload and compute overlap request n's download. Compute is in request
+// order on one stream, so what the stages carry advances pair by pair.
+constexpr int kSlots = 4;
+
 struct Segment {
     uint32_t id = 0;
     int device = 0;
     nxs_geometry g{};
     std::vector<Member> members;
     std::vector<Spec> entries, outputs;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr, upload = nullptr, download = nullptr;
     std::mutex order;  // one request enqueued at a time
+    uint64_t sequence = 0;
     PinnedPool pinned;
-    // device buffers
-    uint8_t *frames[2] = {nullptr, nullptr}, *images[2] = {nullptr, nullptr};
-    float *disparity[2] = {nullptr, nullptr}, *depth_m = nullptr, *grid = nullptr;
-    float *quality_sums = nullptr, *quality_columns = nullptr;
-    uint16_t *depth_mm = nullptr;
-    int32_t *kept = nullptr;
+    Slot slots[kSlots];
+    // shared by every request, touched only on `stream`
+    float *depth_m = nullptr, *quality_columns = nullptr;
     DeviceBuffer scratch;
     std::vector<void *> allocations;
 
@@ -149,10 +166,15 @@ struct Segment {
     }
     ~Segment() {
         cudaSetDevice(device);
-        if (stream) cudaStreamSynchronize(stream);
+        for (cudaStream_t st : {upload, stream, download})
+            if (st) cudaStreamSynchronize(st);
         for (void *p : allocations) cudaFree(p);
         scratch.release();
-        if (stream) cudaStreamDestroy(stream);
+        for (Slot &slot : slots)
+            for (cudaEvent_t ev : {slot.entered, slot.computed, slot.free})
+                if (ev) cudaEventDestroy(ev);
+        for (cudaStream_t st : {upload, stream, download})
+            if (st) cudaStreamDestroy(st);
     }
 };
 
@@ -852,7 +874,9 @@ extern "C" nxs_status nxs_configure(nxs_context *c, uint32_t id, const nxs_geome
         seg->members.push_back(m);
     }
     cudaSetDevice(c->device);
-    cudaError_t e = cudaStreamCreateWithFlags(&seg->stream, cudaStreamNonBlocking);
+    cudaError_t e = cudaSuccess;
+    for (cudaStream_t *st : {&seg->upload, &seg->stream, &seg->download})
+        if (!e) e = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
     const size_t pixels = (size_t)g.width * g.height;
     const size_t frame = (size_t)g.frame_width * g.frame_height;
     int max_disparities = 0, decimation = 1;
@@ -860,17 +884,21 @@ extern "C" nxs_status nxs_configure(nxs_context *c, uint32_t id, const nxs_geome
         if (m.kind == Kind::Disparity) max_disparities = std::max(max_disparities, m.disparities);
         if (m.kind == Kind::Cloud) decimation = m.decimation;
     }
-    if (!e) e = seg->alloc(&seg->frames[0], std::max<size_t>(frame, 1));
-    if (!e) e = seg->alloc(&seg->frames[1], std::max<size_t>(frame, 1));
-    if (!e) e = seg->alloc(&seg->images[0], pixels);
-    if (!e) e = seg->alloc(&seg->images[1], pixels);
-    if (!e) e = seg->alloc(&seg->disparity[0], pixels);
-    if (!e) e = seg->alloc(&seg->disparity[1], pixels);
+    for (Slot &slot : seg->slots) {
+        if (!e) e = seg->alloc(&slot.frames[0], std::max<size_t>(frame, 1));
+        if (!e) e = seg->alloc(&slot.frames[1], std::max<size_t>(frame, 1));
+        if (!e) e = seg->alloc(&slot.images[0], pixels);
+        if (!e) e = seg->alloc(&slot.images[1], pixels);
+        if (!e) e = seg->alloc(&slot.disparity[0], pixels);
+        if (!e) e = seg->alloc(&slot.disparity[1], pixels);
+        if (!e) e = seg->alloc(&slot.depth_mm, pixels);
+        if (!e) e = seg->alloc(&slot.grid, 3 * (pixels / (decimation * decimation) + 1));
+        if (!e) e = seg->alloc(&slot.kept, 1);
+        if (!e) e = seg->alloc(&slot.quality_sums, 5);
+        for (cudaEvent_t *ev : {&slot.entered, &slot.computed, &slot.free})
+            if (!e) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+    }
     if (!e) e = seg->alloc(&seg->depth_m, pixels);
-    if (!e) e = seg->alloc(&seg->depth_mm, pixels);
-    if (!e) e = seg->alloc(&seg->grid, 3 * (pixels / (decimation * decimation) + 1));
-    if (!e) e = seg->alloc(&seg->kept, 1);
-    if (!e) e = seg->alloc(&seg->quality_sums, 5);
     if (!e) e = seg->alloc(&seg->quality_columns, 5 * (size_t)g.width);
     if (!e && max_disparities)
         e = seg->scratch.reserve(matcher_scratch_bytes(g.width, g.height, max_disparities));
@@ -990,18 +1018,25 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
     }
 
     std::lock_guard<std::mutex> order(seg->order);
+    Slot &slot = seg->slots[seg->sequence++ % kSlots];
     cudaStream_t s = seg->stream;
     const size_t pixels = (size_t)g.width * g.height;
-    int current = 0;  // which disparity buffer holds the disparity so far
+    // Upload, once the slot's last request has downloaded its outputs.
+    e = cudaStreamWaitEvent(seg->upload, slot.free, 0);
     for (size_t k = 0; k < seg->entries.size() && !e; ++k) {
         const std::string &name = seg->entries[k].name;
-        void *dst = name == "left_frame" ? (void *)seg->frames[0]
-                    : name == "right_frame" ? (void *)seg->frames[1]
-                    : name == "left"        ? (void *)seg->images[0]
-                    : name == "right"       ? (void *)seg->images[1]
-                                            : (void *)seg->disparity[0];
-        e = cudaMemcpyAsync(dst, staged[k], seg->entries[k].bytes(), cudaMemcpyHostToDevice, s);
+        void *dst = name == "left_frame" ? (void *)slot.frames[0]
+                    : name == "right_frame" ? (void *)slot.frames[1]
+                    : name == "left"        ? (void *)slot.images[0]
+                    : name == "right"       ? (void *)slot.images[1]
+                                            : (void *)slot.disparity[0];
+        e = cudaMemcpyAsync(dst, staged[k], seg->entries[k].bytes(), cudaMemcpyHostToDevice,
+                            seg->upload);
     }
+    if (!e) e = cudaEventRecord(slot.entered, seg->upload);
+    // Compute, in request order.
+    if (!e) e = cudaStreamWaitEvent(s, slot.entered, 0);
+    int current = 0;  // which of the slot's disparity buffers holds the disparity so far
     for (size_t i = 0; i < n && !e; ++i) {
         Member &m = seg->members[i];
         const Live &l = live[i];
@@ -1010,54 +1045,57 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
         switch (m.kind) {
         case Kind::Rectification:
             for (int side = 0; side < 2 && !e; ++side)
-                e = launch_rectify(seg->frames[side], g.frame_width, g.frame_height,
-                                   l.cameras[side], g.width, g.height, seg->images[side], s);
+                e = launch_rectify(slot.frames[side], g.frame_width, g.frame_height,
+                                   l.cameras[side], g.width, g.height, slot.images[side], s);
             break;
         case Kind::Disparity: {
             MatcherScratch ms =
                 carve_matcher_scratch(seg->scratch.ptr, g.width, g.height, m.disparities);
-            e = run_matcher(seg->images[0], seg->images[1], g.width, g.height, m.disparities,
+            e = run_matcher(slot.images[0], slot.images[1], g.width, g.height, m.disparities,
                             m.paths, l.sgm.p1, l.sgm.p2, l.sgm.uniqueness, 1, ms,
-                            seg->disparity[current], s);
+                            slot.disparity[current], s);
             break;
         }
         case Kind::Speckle:
-            e = launch_despeckle(seg->disparity[current], g.width, g.height, l.a, l.b, m.radius,
-                                 seg->disparity[1 - current], s);
+            e = launch_despeckle(slot.disparity[current], g.width, g.height, l.a, l.b, m.radius,
+                                 slot.disparity[1 - current], s);
             current = 1 - current;
             break;
         case Kind::Temporal:
-            e = launch_temporal(seg->disparity[current], m.previous, m.missed, pixels, l.a, l.b,
+            e = launch_temporal(slot.disparity[current], m.previous, m.missed, pixels, l.a, l.b,
                                 l.c, m.max_missed, s);
             break;
         case Kind::Depth:
-            e = launch_depth(seg->disparity[current], pixels, l.a, l.b, seg->depth_mm,
+            e = launch_depth(slot.disparity[current], pixels, l.a, l.b, slot.depth_mm,
                              seg->depth_m, s);
             break;
         case Kind::Cloud:
             e = launch_cloud(seg->depth_m, g.width, g.height, m.decimation, l.a, l.b, l.c,
-                             m.min_depth_m, m.max_depth_m, seg->grid, seg->kept, s);
+                             m.min_depth_m, m.max_depth_m, slot.grid, slot.kept, s);
             break;
         case Kind::Quality:
-            e = launch_quality(seg->disparity[current], m.previous, g.width, g.height,
-                               seg->quality_columns, seg->quality_sums, s);
+            e = launch_quality(slot.disparity[current], m.previous, g.width, g.height,
+                               seg->quality_columns, slot.quality_sums, s);
             break;
         }
     }
     if (!e) e = cudaEventRecord(r->marks[n], s);
+    if (!e) e = cudaEventRecord(slot.computed, s);
     // Download the outputs into the request's pinned blocks.
+    if (!e) e = cudaStreamWaitEvent(seg->download, slot.computed, 0);
     r->outputs.resize(seg->outputs.size());
     r->names.resize(seg->outputs.size());
     for (size_t k = 0; k < seg->outputs.size() && !e; ++k) {
         const Spec &spec = seg->outputs[k];
-        const void *src = spec.name == "left"           ? (const void *)seg->images[0]
-                          : spec.name == "right"        ? (const void *)seg->images[1]
-                          : spec.name == "disparity"    ? (const void *)seg->disparity[current]
-                          : spec.name == "depth_mm"     ? (const void *)seg->depth_mm
-                          : spec.name == "cloud_grid"   ? (const void *)seg->grid
-                          : spec.name == "cloud_points" ? (const void *)seg->kept
-                                                        : (const void *)seg->quality_sums;
-        e = cudaMemcpyAsync(out_host[k], src, spec.bytes(), cudaMemcpyDeviceToHost, s);
+        const void *src = spec.name == "left"           ? (const void *)slot.images[0]
+                          : spec.name == "right"        ? (const void *)slot.images[1]
+                          : spec.name == "disparity"    ? (const void *)slot.disparity[current]
+                          : spec.name == "depth_mm"     ? (const void *)slot.depth_mm
+                          : spec.name == "cloud_grid"   ? (const void *)slot.grid
+                          : spec.name == "cloud_points" ? (const void *)slot.kept
+                                                        : (const void *)slot.quality_sums;
+        e = cudaMemcpyAsync(out_host[k], src, spec.bytes(), cudaMemcpyDeviceToHost,
+                            seg->download);
         r->names[k] = spec.name;
         nxs_tensor &t = r->outputs[k];
         t.name = r->names[k].c_str();
@@ -1067,11 +1105,12 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
         t.data = out_host[k];
         t.bytes = spec.bytes();
     }
-    if (!e) e = cudaEventRecord(r->done, s);
-    if (!e && done) e = cudaLaunchHostFunc(s, request_done, r);
+    if (!e) e = cudaEventRecord(slot.free, seg->download);
+    if (!e) e = cudaEventRecord(r->done, seg->download);
+    if (!e && done) e = cudaLaunchHostFunc(seg->download, request_done, r);
     if (e) {
-        // The stream is still ordered: wait for what was enqueued before freeing.
-        cudaStreamSynchronize(s);
+        // The streams are still ordered: wait for what was enqueued before freeing.
+        for (cudaStream_t st : {seg->upload, seg->stream, seg->download}) cudaStreamSynchronize(st);
         nxs_request_free(r);
         return cuda_status(e, error, error_len, "enqueueing the request");
     }
@@ -1158,6 +1197,6 @@ extern "C" nxs_status nxs_release(nxs_context *c, uint32_t id) {
         c->segments.erase(it);
     }
     cudaSetDevice(c->device);
-    cudaStreamSynchronize(seg->stream);
+    for (cudaStream_t st : {seg->upload, seg->stream, seg->download}) cudaStreamSynchronize(st);
     return NXS_OK;
 }

@@ -165,6 +165,16 @@ def make_camera(k, d, inverse_pr):
     return cam
 
 
+class _PinnedView:
+    """An array interface over a request's pinned output block; holding the
+    request keeps the block from being recycled."""
+
+    def __init__(self, request, address, shape, dtype):
+        self._request = request
+        self.__array_interface__ = {"data": (address, False), "shape": shape,
+                                    "typestr": dtype.str, "version": 3}
+
+
 class Request:
     """A pair sent through a segment: wait for it, then read its outputs."""
 
@@ -188,8 +198,9 @@ class Request:
         _check(status, buf)
         return True
 
-    def outputs(self):
-        """{name: numpy array}, copied out of the request."""
+    def outputs(self, copy=True):
+        """{name: numpy array}. With copy=False the arrays view the request's
+        pinned host memory and keep the request alive until they are dropped."""
         n = ctypes.c_uint32()
         tensors = ctypes.POINTER(Tensor)()
         _check(load().nxs_request_outputs(self._handle, ctypes.byref(n), ctypes.byref(tensors)),
@@ -198,9 +209,8 @@ class Request:
         for i in range(n.value):
             t = tensors[i]
             shape = tuple(t.dims[:t.rank])
-            dtype = DTYPES[t.type]
-            raw = ctypes.string_at(t.data, t.bytes)
-            result[t.name.decode()] = np.frombuffer(raw, dtype=dtype).reshape(shape).copy()
+            view = np.asarray(_PinnedView(self, t.data, shape, np.dtype(DTYPES[t.type])))
+            result[t.name.decode()] = view.copy() if copy else view
         return result
 
     def times_us(self):

@@ -242,12 +242,12 @@ class CudaSegment:
         try:
             if not request.wait(-1 if timeout is None else int(timeout)):
                 return "timeout"
-            outputs = request.outputs()
+            # Views of the request's pinned memory: the request lives as long as they do.
+            outputs = request.outputs(copy=False)
             segment.times_us = request.times_us()
         except native.NativeError as error:
             request.free()
             return ("error", error.message)
-        request.free()
         if "cloud_points" in outputs:
             outputs["cloud_points"] = outputs["cloud_points"].reshape(())
         return ("ok", outputs, segment, time.monotonic_ns())
