@@ -215,11 +215,10 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     native.load()
     ctx = native.Context(local_rank)
-    rig, frames = make_inputs(args.inputs, seed=1 + rank)
+    rig, frames = make_inputs(args.inputs, seed=replicas.seed(rank, 0))
+    from nx_stereo_b200 import replicas
+
     stream_obj = torch.cuda.Stream()
-    dist = world > 1
-    if dist:
-        import torch.distributed as td
 
     with torch.cuda.stream(stream_obj):
         s = stream_obj.cuda_stream
@@ -229,8 +228,7 @@ def run_ours(args, rank, world, local_rank):
         for i in range(args.warmup):
             pipe.step(d_frames[i % len(d_frames)])
         torch.cuda.synchronize()
-        if dist:
-            td.barrier()
+        replicas.barrier()
         sampler = ClockSampler(local_rank if os.environ.get("CUDA_VISIBLE_DEVICES") is None else None)
         sampler.start()
         time.sleep(0.3)
@@ -248,12 +246,8 @@ def run_ours(args, rank, world, local_rank):
         stage_ms = {name: statistics.mean(m[k].elapsed_time(m[k + 1]) for m in marks)
                     for k, name in enumerate(DevicePipeline.STAGES)}
         paths_ms = [m[3].elapsed_time(m[4]) for m in marks]
-    total_s = sum(step_ms) / 1000.0
-    if dist:
-        t = torch.tensor([total_s], device="cuda", dtype=torch.float64)
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        total_s = float(t.item())
-    value = world * args.steps / total_s
+    total_s = replicas.max_over_ranks(sum(step_ms) / 1000.0, device="cuda")
+    value = replicas.whole_job_rate(args.steps, world, total_s)
 
     # e2e: the public API, host frames in, outputs back to the host.
     geometry = segment.standard_geometry(WIDTH, HEIGHT, the_rig=rig)
@@ -287,16 +281,11 @@ def run_ours(args, rank, world, local_rank):
 
     e2e_loop(max(args.warmup, mod.depth()))
     torch.cuda.synchronize()
-    if dist:
-        td.barrier()
+    replicas.barrier()
     e0 = time.perf_counter()
     e2e_loop(args.steps)
     torch.cuda.synchronize()
-    e_s = time.perf_counter() - e0
-    if dist:
-        t = torch.tensor([e_s], device="cuda", dtype=torch.float64)
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        e_s = float(t.item())
+    e_s = replicas.max_over_ranks(time.perf_counter() - e0, device="cuda")
     sampler.stop()
     clocks = sampler.summary(t0, t1)
     seg.release()
@@ -330,7 +319,8 @@ def run_ours(args, rank, world, local_rank):
         "pipeline_roofline": {"b_alg_per_pair": b_alg,
                               "achieved_gbs": round(b_alg * value / world / 1e9, 1),
                               "frac": round(b_alg * value / world / 1e9 / peak, 4)},
-        "e2e": {"value": round(world * args.steps / e_s, 2), "unit": "pairs/s",
+        "e2e": {"value": round(replicas.whole_job_rate(args.steps, world, e_s), 2),
+                "unit": "pairs/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "CudaSegment.send_request/await_ (C ABI nxs_run_async), depth "
                        f"{mod.depth()}"},
@@ -386,24 +376,20 @@ def run_reference(args):
 
 
 def main():
+    from nx_stereo_b200 import replicas
+
     args = parse()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local_rank = replicas.ranks()
     if args.impl == "reference":
         if rank != 0:
             return 0
         print(json.dumps(run_reference(args)))
         return 0
     if world > 1:
-        import datetime
-
         import torch
-        import torch.distributed as td
 
         torch.cuda.set_device(local_rank)
-        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                              device_id=torch.device("cuda", local_rank))
+        replicas.init("nccl", device=torch.device("cuda", local_rank))
     line = run_ours(args, rank, world, local_rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
@@ -416,7 +402,7 @@ def main():
     if world > 1:
         import torch.distributed as td
 
-        td.barrier()
+        replicas.barrier()
         td.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
