@@ -210,14 +210,12 @@ class DevicePipeline:
 def run_ours(args, rank, world, local_rank):
     import torch
 
-    from nx_stereo_b200 import native, segment, stage
+    from nx_stereo_b200 import native, replicas, segment, stage
 
     torch.cuda.set_device(local_rank)
     native.load()
     ctx = native.Context(local_rank)
     rig, frames = make_inputs(args.inputs, seed=replicas.seed(rank, 0))
-    from nx_stereo_b200 import replicas
-
     stream_obj = torch.cuda.Stream()
 
     with torch.cuda.stream(stream_obj):

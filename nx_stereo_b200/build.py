@@ -7,6 +7,7 @@ it travels with the sources; nvcc cross-compiles without a GPU.
 its own as the reference evaluates it (the kernels also spell those steps
 with __f*_rn intrinsics).
 """
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -16,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBRARY = os.path.join(HERE, "libnxs_b200.so")
 SOURCES = ["matcher.cu", "stages.cu", "abi.cu", "matcher_static.cu"]
-HEADERS = ["nxs_device.cuh", "nxs_kernels.h"]
+HEADERS = ["nxs_device.cuh", "nxs_kernels.h", "nxs_matcher.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-fmad=false", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr"]
@@ -36,15 +37,18 @@ def build(force=False, verbose=False):
         return LIBRARY
     build_dir = os.path.join(HERE, "_build")
     os.makedirs(build_dir, exist_ok=True)
-    objects = []
+    commands, objects = [], []
     for source in SOURCES:
         obj = os.path.join(build_dir, source.replace(".cu", ".o"))
         cmd = [NVCC] + FLAGS + ["-c", os.path.join(CSRC, source), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        commands.append(cmd)
         objects.append(obj)
+    with concurrent.futures.ThreadPoolExecutor(len(commands)) as pool:
+        for done in pool.map(lambda c: subprocess.run(c, check=True), commands):
+            pass
     tmp = LIBRARY + ".tmp"
     subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp]
                    + objects + ["-lcudart_static", "-lrt", "-ldl", "-lpthread"], check=True)

@@ -1,0 +1,518 @@
+// Device building blocks of the matcher, shared by the single-pair kernels
+// (matcher.cu) and the batched ones (batch.cu): each takes the pair's buffers
+// and sizes as arguments and the position of its block within the pair.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "nxs_device.cuh"
+
+namespace nxs {
+
+// ---------------------------------------------------------------- census
+// 9x7 sparse census (lib/nx_stereo.ex:491-505): bit i for the i-th neighbour
+// in row-major order over dy in -3..3, dx in -4..4, both non-zero, set where
+// neighbour + 1 < centre; borders replicated (lib/nx_stereo/image.ex:508-537).
+// A 32x8 block stages its window of 40x14 pixels in shared memory.
+constexpr int kCensusX = 32, kCensusY = 8;
+
+__device__ __forceinline__ void census_tile(const uint8_t *__restrict__ image, int width,
+                                            int height, uint64_t *__restrict__ codes, int x0,
+                                            int y0) {
+    __shared__ uint8_t tile[kCensusY + 6][kCensusX + 8];
+    const int tid = threadIdx.y * kCensusX + threadIdx.x;
+    for (int i = tid; i < (kCensusY + 6) * (kCensusX + 8); i += kCensusX * kCensusY) {
+        int ty = i / (kCensusX + 8), tx = i % (kCensusX + 8);
+        int sy = min(max(y0 + ty - 3, 0), height - 1);
+        int sx = min(max(x0 + tx - 4, 0), width - 1);
+        tile[ty][tx] = image[(size_t)sy * width + sx];
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    if (x >= width || y >= height) return;
+    const int centre = tile[threadIdx.y + 3][threadIdx.x + 4];
+    uint64_t code = 0;
+    int bit = 0;
+#pragma unroll
+    for (int dy = -3; dy <= 3; ++dy) {
+        if (dy == 0) continue;
+#pragma unroll
+        for (int dx = -4; dx <= 4; ++dx) {
+            if (dx == 0) continue;
+            int n = tile[threadIdx.y + 3 + dy][threadIdx.x + 4 + dx];
+            code |= (uint64_t)(n + 1 < centre) << bit;
+            ++bit;
+        }
+    }
+    codes[(size_t)y * width + x] = code;
+}
+
+// ---------------------------------------------------------------- costs
+// costs[y][x][d] = popcount(left[y][x] ^ right[y][x - d]), right codes left of
+// the image zero (lib/nx_stereo.ex:528-542). A block of 128 threads covers 64
+// pixels of a row. It stages their left codes and the D + 63 right codes they
+// reach; a thread computes 4 neighbouring pixels x 16 disparities, whose right
+// codes are 19 consecutive ones held in registers, into a shared tile, and the
+// block then writes its 64 x D bytes out contiguously with 16-byte stores.
+constexpr int kCostPixels = 64;
+
+__host__ __device__ inline size_t costs_shared_bytes(int disparities) {
+    return sizeof(uint64_t) * (2 * kCostPixels + disparities) +
+           (size_t)kCostPixels * (disparities + 16);
+}
+
+__device__ __forceinline__ void costs_tile(const uint64_t *__restrict__ left_codes,
+                                           const uint64_t *__restrict__ right_codes, int width,
+                                           int disparities, uint8_t *__restrict__ costs, int x0,
+                                           int y, uint8_t *staged) {
+    const int D = disparities, pitch = D + 16;  // tile row pitch: 16-byte stores spread banks
+    uint64_t *lefts = reinterpret_cast<uint64_t *>(staged);
+    uint64_t *rights = lefts + kCostPixels;
+    uint8_t *tile = staged + sizeof(uint64_t) * (2 * kCostPixels + D);
+    const size_t row = (size_t)y * width;
+    for (int i = threadIdx.x; i < kCostPixels; i += blockDim.x)
+        lefts[i] = x0 + i < width ? left_codes[row + x0 + i] : 0;
+    for (int i = threadIdx.x; i < kCostPixels + D - 1; i += blockDim.x) {
+        const int x = x0 - (D - 1) + i;
+        rights[i] = (x >= 0 && x < width) ? right_codes[row + x] : 0;
+    }
+    __syncthreads();
+    const int groups = kCostPixels / 4, chunks = D / 16;
+    for (int t = threadIdx.x; t < groups * chunks; t += blockDim.x) {
+        const int p0 = 4 * (t % groups), d0 = 16 * (t / groups);
+        // pixel p0 + i at disparity d0 + k reads rights[p0 + i - d0 - k + D - 1]
+        //                                     = window[i - k + 15]
+        const uint64_t *base = rights + p0 - d0 + D - 16;
+        uint64_t window[19];
+#pragma unroll
+        for (int j = 0; j < 19; ++j) window[j] = base[j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint64_t l = lefts[p0 + i];
+            uint32_t words[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                uint32_t w = 0;
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+                    w |= (uint32_t)__popcll(l ^ window[i - (4 * q + b) + 15]) << (8 * b);
+                words[q] = w;
+            }
+            *reinterpret_cast<uint4 *>(tile + (p0 + i) * pitch + d0) =
+                make_uint4(words[0], words[1], words[2], words[3]);
+        }
+    }
+    __syncthreads();
+    const int pixels = min(kCostPixels, width - x0);
+    uint4 *out = reinterpret_cast<uint4 *>(costs + (row + x0) * D);
+    for (int c = threadIdx.x; c < pixels * chunks; c += blockDim.x)
+        out[c] = *reinterpret_cast<const uint4 *>(tile + (c / chunks) * pitch + (c % chunks) * 16);
+}
+
+// ---------------------------------------------------------------- paths
+// libSGM's normalised recurrence (lib/nx_stereo.ex:575-606) along every scan
+// line of every direction, unnormalised:
+//   L[d] = min(prev[d], prev[d-1] + p1, prev[d+1] + p1, m + p2) - m + C[d],
+//   m = min over d of prev,
+// which equals the reference's min(min(a, p2), min(a[d-1], a[d+1]) + p1) + C
+// with a = prev - m; its out-of-range neighbours (p2 - p1, so p2 once p1 is
+// added) never beat m + p2, so they read as +inf. Lanes past D hold +inf.
+// A path starts from zero where it enters the image, so its first step is C.
+//
+// A group of G lanes follows one line, each lane holding 2 * WORDS
+// disparities as u16x2 words (five integer instructions per word and step),
+// and a warp follows 32 / G lines in lockstep. Each lane copies its costs for the next kPrefetch - 1 steps into a shared
+// ring with cp.async while a step computes, and stores its path costs with
+// 16-byte stores.
+constexpr int kPrefetch = 8;
+
+struct PathSetup {
+    int width, height, disparities, p1, p2, paths;
+    int first_warp[9];  // first warp of each direction; first_warp[paths] = total
+    int lines[8];       // scan lines of each direction
+    int dy[8], dx[8];
+    int order[8];       // direction of each slot: rows first, then columns, then diagonals
+    int straight;       // slots of rows and columns
+    size_t volume;      // bytes of one direction's volume
+};
+
+__device__ __forceinline__ void unpack16(const uint4 c, uint32_t *w) {
+    w[0] = __byte_perm(c.x, 0, 0x4140);
+    w[1] = __byte_perm(c.x, 0, 0x4342);
+    w[2] = __byte_perm(c.y, 0, 0x4140);
+    w[3] = __byte_perm(c.y, 0, 0x4342);
+    w[4] = __byte_perm(c.z, 0, 0x4140);
+    w[5] = __byte_perm(c.z, 0, 0x4342);
+    w[6] = __byte_perm(c.w, 0, 0x4140);
+    w[7] = __byte_perm(c.w, 0, 0x4342);
+}
+
+__device__ __forceinline__ uint4 pack16(const uint32_t *w) {
+    return make_uint4(__byte_perm(w[0], w[1], 0x6420), __byte_perm(w[2], w[3], 0x6420),
+                      __byte_perm(w[4], w[5], 0x6420), __byte_perm(w[6], w[7], 0x6420));
+}
+
+// The start and length of scan line `line` of direction (dy, dx): rows run
+// along x, columns along y, and a diagonal enters from the first row it meets
+// (line < W) or from the side column it meets.
+__device__ __forceinline__ int line_start(int line, int dy, int dx, int W, int H, int *y0,
+                                          int *x0) {
+    if (dy == 0) {
+        *y0 = line;
+        *x0 = dx > 0 ? 0 : W - 1;
+        return W;
+    }
+    if (dx == 0) {
+        *x0 = line;
+        *y0 = dy > 0 ? 0 : H - 1;
+        return H;
+    }
+    if (line < W) {
+        *x0 = line;
+        *y0 = dy > 0 ? 0 : H - 1;
+    } else {
+        *x0 = dx > 0 ? 0 : W - 1;
+        const int k = line - W + 1;
+        *y0 = dy > 0 ? k : H - 1 - k;
+    }
+    const int rows = dy > 0 ? H - *y0 : *y0 + 1;
+    const int columns = dx > 0 ? W - *x0 : *x0 + 1;
+    return min(rows, columns);
+}
+
+// 16-byte global -> shared copies that complete asynchronously (cp.async);
+// src_size 0 zero-fills without reading.
+__device__ __forceinline__ void copy16_async(void *shared, const void *global, bool valid) {
+    const unsigned address = (unsigned)__cvta_generic_to_shared(shared);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(address), "l"(global),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void copy_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void copy_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// The lines of one warp: G lanes per line, WORDS u16x2 words per lane.
+// `ring` is this thread's kPrefetch x (WORDS / 8) slots of 16 bytes, strided
+// by THREADS threads.
+template <int G, int WORDS, bool FULL, int THREADS>
+__device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
+                                             uint8_t *__restrict__ out, const PathSetup &s,
+                                             int p, int line, int member, uint4 *ring) {
+    constexpr int CHUNKS = WORDS / 8;  // 16-byte chunks per lane
+    const int dy = s.dy[p], dx = s.dx[p];
+    const int W = s.width, H = s.height, D = s.disparities;
+    int y0 = 0, x0 = 0, length = 0;
+    if (line < s.lines[p]) length = line_start(line, dy, dx, W, H, &y0, &x0);
+    const bool active = FULL || member * 2 * WORDS < D;
+    const ptrdiff_t stride = ((ptrdiff_t)dy * W + dx) * D;
+    const size_t at = ((size_t)y0 * W + x0) * D + member * 2 * WORDS;
+    const uint8_t *ahead = costs + at;
+    uint8_t *dst = out + (size_t)p * s.volume + at;
+    const int steps = (int)__reduce_max_sync(kFullMask, (unsigned)length);
+
+    uint32_t r[WORDS];
+#pragma unroll
+    for (int k = 0; k < WORDS; ++k) r[k] = active ? 0u : kInf2;
+    uint32_t m2 = 0, j2 = (uint32_t)s.p2 * 0x10001u;
+    const uint32_t p1x2 = (uint32_t)s.p1 * 0x10001u, p2x2 = (uint32_t)s.p2 * 0x10001u;
+
+#pragma unroll
+    for (int i = 0; i < kPrefetch - 1; ++i) {
+        const bool valid = active && i < length;
+#pragma unroll
+        for (int c = 0; c < CHUNKS; ++c)
+            copy16_async(ring + (i * CHUNKS + c) * THREADS, valid ? ahead + 16 * c : costs, valid);
+        copy_commit();
+        ahead += stride;
+    }
+    for (int base = 0; base < steps; base += kPrefetch) {
+#pragma unroll
+        for (int i = 0; i < kPrefetch; ++i) {
+            const int step = base + i;
+            if (step >= steps) break;  // uniform across the warp
+            {   // the copy of step + kPrefetch - 1 goes to the slot read last step
+                const bool valid = active && step + kPrefetch - 1 < length;
+                const int slot = (i + kPrefetch - 1) % kPrefetch;
+#pragma unroll
+                for (int c = 0; c < CHUNKS; ++c)
+                    copy16_async(ring + (slot * CHUNKS + c) * THREADS,
+                                 valid ? ahead + 16 * c : costs, valid);
+                copy_commit();
+                ahead += stride;
+            }
+            copy_wait<kPrefetch - 1>();
+            uint32_t cost[WORDS];
+#pragma unroll
+            for (int c = 0; c < CHUNKS; ++c) unpack16(ring[(i * CHUNKS + c) * THREADS], cost + 8 * c);
+            uint32_t from_left = __shfl_up_sync(kFullMask, r[WORDS - 1], 1);
+            uint32_t from_right = __shfl_down_sync(kFullMask, r[0], 1);
+            if (member == 0) from_left = kInf2;
+            if (member == G - 1) from_right = kInf2;
+            uint32_t shifted[WORDS + 1];  // shifted[k]: the (d - 1) values of word k
+            shifted[0] = __byte_perm(from_left, r[0], 0x5432);
+#pragma unroll
+            for (int k = 1; k < WORDS; ++k) shifted[k] = __byte_perm(r[k - 1], r[k], 0x5432);
+            shifted[WORDS] = __byte_perm(r[WORDS - 1], from_right, 0x5432);
+#pragma unroll
+            for (int k = 0; k < WORDS; ++k) {
+                const uint32_t neighbour = vmin2(shifted[k], shifted[k + 1]);
+                uint32_t t = vmin2(r[k], j2);
+                t = __viaddmin_u16x2(neighbour, p1x2, t);
+                // t >= m in both halves, so the subtraction borrows nowhere.
+                const uint32_t value = t - m2 + cost[k];
+                r[k] = (FULL || active) ? value : kInf2;
+            }
+            if (active && step < length) {
+#pragma unroll
+                for (int c = 0; c < CHUNKS; ++c)
+                    *reinterpret_cast<uint4 *>(dst + 16 * c) = pack16(r + 8 * c);
+            }
+            dst += stride;
+            uint32_t lowest = __vimin3_u16x2(r[0], r[1], r[2]);
+#pragma unroll
+            for (int k = 3; k + 1 < WORDS; k += 2) lowest = __vimin3_u16x2(lowest, r[k], r[k + 1]);
+            if (WORDS % 2 == 0) lowest = vmin2(lowest, r[WORDS - 1]);
+            uint32_t m = min(lowest & 0xFFFFu, lowest >> 16);
+#pragma unroll
+            for (int offset = G / 2; offset >= 1; offset /= 2)
+                m = min(m, __shfl_xor_sync(kFullMask, m, offset));
+            m2 = m * 0x10001u;
+            j2 = m2 + p2x2;
+        }
+    }
+    copy_wait<0>();
+}
+
+// The scan line of direction (dy, dx) with rank `rank` when the lines are
+// ordered by length, longest first, so the lines a warp follows together are
+// alike in length. Rows and columns are all alike. A diagonal line either
+// starts on the first row it meets, at a distance j = 1..W from the side it
+// runs away from (length min(H, j)), or on a side column at row offset
+// k = 1..H-1 (length min(H - k, W)).
+__device__ __forceinline__ int ranked_line(int rank, int dy, int dx, int W, int H) {
+    if (dy == 0 || dx == 0) return rank;
+    const int full = (W > H ? W - H : H - W) + 1;  // lines of the greatest length
+    int j = 0, k = 0;                              // first-row distance, or side offset
+    if (rank < full) {
+        if (W >= H) j = W - rank;
+        else if (rank < full - 1) k = rank + 1;
+        else j = W;
+    } else {
+        const int q = rank - full;
+        const int len = min(W, H) - 1 - q / 2;
+        if (q % 2 == 0) j = len;
+        else k = H - len;
+    }
+    if (j > 0) return dx > 0 ? W - j : j - 1;
+    return W - 1 + k;
+}
+
+
+// One warp's lines: warp `warp` of the pair's path launch, lane `lane`.
+// Rows, then columns, then the diagonals of all four directions by rank.
+template <int G, bool FULL>
+__device__ __forceinline__ void path_warp(const uint8_t *__restrict__ costs,
+                                          uint8_t *__restrict__ paths_out, const PathSetup &s,
+                                          int warp, int lane, uint4 *ring) {
+    int slot = 0;
+    while (warp >= s.first_warp[slot + 1]) ++slot;
+    int p, group;
+    if (slot < s.straight) {  // rows and columns, direction by direction
+        p = s.order[slot];
+        group = warp - s.first_warp[slot];
+    } else {                  // diagonals interleaved, longest first
+        const int w = warp - s.first_warp[s.straight];
+        const int diagonals = s.paths - s.straight;
+        p = s.order[s.straight + w % diagonals];
+        group = w / diagonals;
+    }
+    const int rank = group * (32 / G) + lane / G;
+    const int line =
+        rank < s.lines[p] ? ranked_line(rank, s.dy[p], s.dx[p], s.width, s.height) : rank;
+    follow_lines<G, 8, FULL, 32>(costs, paths_out, s, p, line, lane % G, ring);
+}
+
+// Lanes per line (paths) or per pixel (selection), 16 disparities each: a
+// power of two.
+__host__ __device__ inline int group_lanes(int disparities) {
+    return disparities <= 64 ? 4 : (disparities <= 128 ? 8 : 16);
+}
+
+// ---------------------------------------------------------------- select
+// Winner, uniqueness and subpixel (lib/nx_stereo.ex:608-641). A group of G
+// lanes takes one pixel, each lane 16 disparities, so a warp takes 32 / G
+// pixels. values = sum of the path costs + 0x8000 past x; the winner is the
+// lowest (value << 16 | d), so ties go to the lowest d; `second` is the
+// lowest value more than one disparity from the winner; the f32 steps are
+// rounded one at a time in the reference's order. Two path volumes add as
+// bytes without carry (127 + 127 < 256) before widening to u16x2.
+template <int G, int PATHS>  // PATHS 0: read u16 sums instead of path volumes
+__device__ __forceinline__ void select_pixels(const void *__restrict__ source, int width,
+                                              int height, int disparities, size_t volume,
+                                              float uniqueness, float *__restrict__ disparity,
+                                              uint32_t *__restrict__ keys, size_t block) {
+    constexpr int PIXELS = 128 / G;  // per block of 128 threads
+    __shared__ __align__(16) uint16_t values_of[PIXELS][256];
+    const int slot = threadIdx.x / G, member = threadIdx.x % G;
+    const size_t pixel = block * PIXELS + slot;
+    const bool valid = pixel < (size_t)width * height;
+    const int D = disparities;
+    const bool active = valid && member * 16 < D;
+    const int x = valid ? (int)(pixel % width) : 0;
+    const int d0 = member * 16;
+    uint32_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = 0;
+    if (active) {
+        const size_t at = pixel * D + d0;
+        if (PATHS == 0) {
+            const uint4 *sums = reinterpret_cast<const uint4 *>(static_cast<const uint16_t *>(source) + at);
+            const uint4 a = sums[0], b = sums[1];
+            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+            v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+        } else {
+            const uint8_t *volumes = static_cast<const uint8_t *>(source) + at;
+            uint4 loaded[PATHS > 0 ? PATHS : 1];
+#pragma unroll
+            for (int p = 0; p < PATHS; ++p)  // every volume's load in flight at once
+                loaded[p] = __ldg(reinterpret_cast<const uint4 *>(volumes + p * volume));
+#pragma unroll
+            for (int p = 0; p < PATHS; p += 2) {
+                const uint4 a = loaded[p];
+                const uint4 b = p + 1 < PATHS ? loaded[p + 1] : make_uint4(0, 0, 0, 0);
+                uint32_t pair[8];
+                unpack16(make_uint4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w), pair);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) v[k] += pair[k];
+            }
+        }
+        if (x < d0 + 15) {  // disparities past the left edge lose
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                v[k] += (d0 + 2 * k > x ? 0x8000u : 0u) | (d0 + 2 * k + 1 > x ? 0x80000000u : 0u);
+        }
+        *reinterpret_cast<uint4 *>(&values_of[slot][d0]) = make_uint4(v[0], v[1], v[2], v[3]);
+        *reinterpret_cast<uint4 *>(&values_of[slot][d0 + 8]) = make_uint4(v[4], v[5], v[6], v[7]);
+    }
+    uint32_t best = 0xFFFFFFFFu;
+    if (active) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t d = (uint32_t)(d0 + 2 * k) | ((uint32_t)(d0 + 2 * k + 1) << 16);
+            best = min(best, min(__byte_perm(v[k], d, 0x1054), __byte_perm(v[k], d, 0x3276)));
+        }
+    }
+#pragma unroll
+    for (int offset = G / 2; offset >= 1; offset /= 2)
+        best = min(best, __shfl_xor_sync(kFullMask, best, offset));
+    const uint32_t minimum = best >> 16;
+    const int winner = (int)(best & 0xFFFFu);
+    uint32_t second = 0xFFFFFFFFu;
+    if (active) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int d = d0 + 2 * k;
+            // d outside [winner - 1, winner + 1]
+            if ((unsigned)(d - winner + 1) > 2u) second = min(second, v[k] & 0xFFFFu);
+            if ((unsigned)(d + 1 - winner + 1) > 2u) second = min(second, v[k] >> 16);
+        }
+    }
+#pragma unroll
+    for (int offset = G / 2; offset >= 1; offset /= 2)
+        second = min(second, __shfl_xor_sync(kFullMask, second, offset));
+    __syncwarp();
+    if (member != 0 || !valid) return;
+    const uint32_t lower = values_of[slot][max(winner - 1, 0)];
+    const uint32_t upper = values_of[slot][min(winner + 1, D - 1)];
+    const float lower_f = (float)lower, upper_f = (float)upper, minimum_f = (float)minimum;
+    // With no disparity outside the winner's neighbours the reference's
+    // minimum is i32::MAX (lib/nx_stereo.ex:620-622).
+    const float second_f = second == 0xFFFFFFFFu ? 2147483647.0f : (float)second;
+    const bool accepted = second_f > fmul(minimum_f, uniqueness);
+    const float denominator = fsub(fadd(lower_f, upper_f), fmul(2.0f, minimum_f));
+    const float bounded = denominator > 1.0f ? denominator : 1.0f;
+    float correction = fdiv(fsub(lower_f, upper_f), fmul(2.0f, bounded));
+    correction = correction < -0.5f ? -0.5f : (correction > 0.5f ? 0.5f : correction);
+    const bool refine = denominator > 0.0f && winner > 0 && winner < min(D - 1, x);
+    const float value_f = refine ? fadd((float)winner, correction) : (float)winner;
+    disparity[pixel] = accepted ? value_f : -1.0f;
+    keys[pixel] = accepted ? ((minimum << 16) | (uint32_t)winner) : kInvalidKey;
+}
+
+// ---------------------------------------------------------------- check
+// OpenCV's left-right check (lib/nx_stereo.ex:643-683), one block per row:
+// the right map is the per-row atomicMin of (key & 0xFFFF0000) | (65535 - d)
+// at x - d, so the cheapest match wins and ties go to the larger d.
+// `right` is the block's shared array of `width` words.
+__device__ __forceinline__ void consistency_row(const float *__restrict__ disparity,
+                                                const uint32_t *__restrict__ keys, int width,
+                                                float *__restrict__ checked, int y,
+                                                uint32_t *right) {
+    const size_t row = (size_t)y * width;
+    for (int x = threadIdx.x; x < width; x += blockDim.x) right[x] = kInvalidKey;
+    __syncthreads();
+    for (int x = threadIdx.x; x < width; x += blockDim.x) {
+        uint32_t key = keys[row + x];
+        if (key == kInvalidKey) continue;
+        int winner = (int)(key & 0xFFFFu);
+        if (x - winner < 0) continue;  // a winner is at most x (past-edge costs lose)
+        atomicMin(&right[x - winner], (key & 0xFFFF0000u) | (65535u - (uint32_t)winner));
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < width; x += blockDim.x) {
+        float value = disparity[row + x];
+        int low = (int)floorf(value), high = (int)ceilf(value);
+        bool rejected = true;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            int d = k == 0 ? low : high;
+            int rx = x - d;
+            bool inside = rx >= 0 && rx < width;
+            uint32_t found = right[min(max(rx, 0), width - 1)];
+            int right_d = 65535 - (int)(found & 0xFFFFu);
+            bool disagrees = inside && found != kInvalidKey && abs(right_d - d) > 1;
+            rejected = rejected && disagrees;
+        }
+        checked[row + x] = (value >= 0.0f && !rejected) ? value : -1.0f;
+    }
+}
+
+// ---------------------------------------------------------------- median
+// Devillard's 9-element network (lib/nx_stereo/image.ex:272, 483-505): the
+// median ends in slot 4; borders replicated. Then, for Stage.Disparity,
+// disparity <= 0 becomes -1 (lib/nx_stereo/stage/disparity.ex:162).
+__device__ __forceinline__ void exchange(float &a, float &b) {
+    const float lo = fminf(a, b), hi = fmaxf(a, b);
+    a = lo;
+    b = hi;
+}
+
+__device__ __forceinline__ void median_at(const float *__restrict__ image, int width,
+                                          int height, int stage_mask,
+                                          float *__restrict__ filtered, int x, int y) {
+    if (x >= width) return;
+    float v[9];
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+            int sy = min(max(y + dy, 0), height - 1), sx = min(max(x + dx, 0), width - 1);
+            v[(dy + 1) * 3 + dx + 1] = image[(size_t)sy * width + sx];
+        }
+    exchange(v[1], v[2]); exchange(v[4], v[5]); exchange(v[7], v[8]);
+    exchange(v[0], v[1]); exchange(v[3], v[4]); exchange(v[6], v[7]);
+    exchange(v[1], v[2]); exchange(v[4], v[5]); exchange(v[7], v[8]);
+    exchange(v[0], v[3]); exchange(v[5], v[8]); exchange(v[4], v[7]);
+    exchange(v[3], v[6]); exchange(v[1], v[4]); exchange(v[2], v[5]);
+    exchange(v[4], v[7]); exchange(v[4], v[2]); exchange(v[6], v[4]);
+    exchange(v[4], v[2]);
+    float out = v[4];
+    if (stage_mask && !(out > 0.0f)) out = -1.0f;
+    filtered[(size_t)y * width + x] = out;
+}
+
+}  // namespace nxs
