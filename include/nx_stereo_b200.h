@@ -311,6 +311,91 @@ nxs_status nxs_cloud_device(const float *d_depth_m, uint32_t width, uint32_t hei
 nxs_status nxs_quality_device(const float *d_disparity, float *d_previous, uint32_t width,
                               uint32_t height, float *d_sums, void *stream);
 
+
+/* ------------------------------------------------------------------------ */
+/* Layer 3: batched matching                                                 */
+/*
+ * Many rectified pairs of uneven size and disparity range matched in one
+ * persistent, graph-captured launch: NxStereo.sgm/3 (lib/nx_stereo.ex:64-74)
+ * on each pair, with Stage.Disparity's mask where a pair asks for it, bit for
+ * bit as nxs_sgm gives it. The reference matches pairs one call at a time
+ * (Matcher::disparity, native/stereo_match/src/lib.rs:105-124); a batch is
+ * planned once (buffers, work queue, graphs) and run many times.
+ */
+typedef struct nxs_batch nxs_batch;
+
+typedef struct {
+    uint32_t width, height;
+    nxs_sgm_params params;
+} nxs_batch_pair;
+
+/* Shapes of the batched launch, which nx_stereo_b200.batch's autotuner picks. */
+typedef struct {
+    int32_t blocks_per_sm;  /* resident blocks of 128 threads per SM, 1..16 */
+    int32_t cost_rows;      /* rows of 64 pixels per costs item, 1..64 */
+    int32_t select_passes;  /* 128 / lanes pixels per pass, passes per selection item */
+    int32_t group_pairs;    /* pairs a group of the queue's pipeline holds, 1..1024 */
+    float quantum_us;       /* whole-GPU microseconds of one run of a phase in the queue */
+    int32_t order;          /* 0: the group pipeline; 1: each phase over all pairs in turn */
+} nxs_batch_tuning;
+
+typedef struct {
+    uint32_t pairs, items, runs, blocks;
+    uint64_t shared_bytes, device_bytes, input_bytes, output_bytes;
+} nxs_batch_stats;
+
+void nxs_batch_default_tuning(nxs_batch_tuning *tuning);
+
+/* Plans a batch: every pair is checked as nxs_sgm_check does; the device
+ * memory of all pairs is allocated at once (NXS_BAD_ARGUMENT when it does not
+ * fit); `tuning` may be NULL for the defaults. */
+nxs_status nxs_batch_create(nxs_context *context, uint32_t n_pairs, const nxs_batch_pair *pairs,
+                            const nxs_batch_tuning *tuning, nxs_batch **batch, char *error,
+                            size_t error_len);
+
+/* Pair `pair`'s images and disparity: in pinned host memory (device_side 0),
+ * which nxs_batch_run copies in and out, or on the device (device_side 1). */
+nxs_status nxs_batch_buffers(nxs_batch *batch, uint32_t pair, int32_t device_side,
+                             uint8_t **left, uint8_t **right, float **disparity);
+
+/* Re-plans the batch for other shapes (the buffers and their contents stay). */
+nxs_status nxs_batch_retune(nxs_batch *batch, const nxs_batch_tuning *tuning, char *error,
+                            size_t error_len);
+
+/* Matches every pair: the host images in, one launch, the disparities out.
+ * Synchronous; NXS_TIMEOUT if a wait inside the launch ran out. */
+nxs_status nxs_batch_run(nxs_batch *batch, char *error, size_t error_len);
+
+/* Enqueues one run on `stream` (NULL: the batch's own stream) without
+ * waiting: with host_buffers, the copies in and out are part of it;
+ * otherwise the device buffers are used as they are. */
+nxs_status nxs_batch_launch(nxs_batch *batch, int32_t host_buffers, void *stream, char *error,
+                            size_t error_len);
+
+/* After a launch has finished: NXS_TIMEOUT if a wait inside it ran out. */
+nxs_status nxs_batch_check(nxs_batch *batch, char *error, size_t error_len);
+
+nxs_status nxs_batch_info(const nxs_batch *batch, nxs_batch_stats *stats);
+
+/* Where the last launch spent its blocks' time (call it once the launch has
+ * finished; the batch's own stream is waited for), in SM cycles summed over
+ * blocks, 16 values: cycles[k] for the items of phase k (census, costs,
+ * paths, selection, check, median), cycles[6 + k] for phase k's items
+ * waiting for phase k - 1, cycles[12] taking items from the queue. */
+nxs_status nxs_batch_clocks(nxs_batch *batch, uint64_t *cycles);
+
+/* The work queue nxs_batch_create would lay out, computed on the host only:
+ * items[6 * i + k] is the number of items of phase k (census, costs, paths,
+ * selection, check, median) of pair i, and each run r of the queue is
+ * runs[4r..4r+3] = (first queue position, pair, phase, first item of the
+ * phase); a run ends where the next begins, the last at the total. Runs are
+ * written when `capacity` holds them all; *n_runs is always set. */
+nxs_status nxs_batch_queue(uint32_t n_pairs, const nxs_batch_pair *pairs,
+                           const nxs_batch_tuning *tuning, uint32_t *items, uint32_t *runs,
+                           uint32_t capacity, uint32_t *n_runs, char *error, size_t error_len);
+
+void nxs_batch_destroy(nxs_batch *batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -188,6 +188,8 @@ struct nxs_context {
     DeviceBuffer scratch, io;
 };
 
+int nxs::context_device(nxs_context *context) { return context->device; }
+
 struct nxs_request {
     std::shared_ptr<Segment> segment;
     std::vector<void *> pinned;  // returned to the segment's pool on free

@@ -22,9 +22,11 @@ __global__ void __launch_bounds__(kCensusX *kCensusY)
     census_kernel(const uint8_t *__restrict__ left, const uint8_t *__restrict__ right, int width,
                   int height, uint64_t *__restrict__ left_codes,
                   uint64_t *__restrict__ right_codes) {
-    census_tile(blockIdx.z == 0 ? left : right, width, height,
-                blockIdx.z == 0 ? left_codes : right_codes, blockIdx.x * kCensusX,
-                blockIdx.y * kCensusY);
+    __shared__ uint8_t tile[census_tile_bytes(kCensusY)];
+    census_tile<kCensusY, kCensusX * kCensusY>(
+        blockIdx.z == 0 ? left : right, width, height,
+        blockIdx.z == 0 ? left_codes : right_codes, blockIdx.x * kCensusX, blockIdx.y * kCensusY,
+        threadIdx.y * kCensusX + threadIdx.x, tile);
 }
 
 cudaError_t launch_census(const uint8_t *left, const uint8_t *right, int width, int height,
@@ -149,8 +151,9 @@ __global__ void __launch_bounds__(128)
     select_kernel(const void *__restrict__ source, int width, int height, int disparities,
                   size_t volume, float uniqueness, float *__restrict__ disparity,
                   uint32_t *__restrict__ keys) {
+    __shared__ __align__(16) uint16_t values_of[128 / G][256];
     select_pixels<G, PATHS>(source, width, height, disparities, volume, uniqueness, disparity,
-                            keys, blockIdx.x);
+                            keys, nullptr, blockIdx.x, values_of);
 }
 
 template <int PATHS>

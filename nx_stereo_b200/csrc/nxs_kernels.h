@@ -6,6 +6,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+struct nxs_context;
+
 namespace nxs {
 
 // Directions in the reference's order (lib/nx_stereo.ex:566-570,
@@ -79,5 +81,12 @@ cudaError_t run_matcher(const uint8_t *left, const uint8_t *right, int width, in
                         int disparities, int paths, int p1, int p2, float uniqueness,
                         int stage_mask, const MatcherScratch &scratch, float *disparity,
                         cudaStream_t stream);
+
+// The device a context was opened on.
+int context_device(nxs_context *context);
+
+// The warp layout of one pair's path launch; returns the number of warps.
+int path_setup(int width, int height, int disparities, int paths, int p1, int p2,
+               struct PathSetup *setup);
 
 }  // namespace nxs

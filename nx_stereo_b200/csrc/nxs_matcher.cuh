@@ -14,38 +14,47 @@ namespace nxs {
 // 9x7 sparse census (lib/nx_stereo.ex:491-505): bit i for the i-th neighbour
 // in row-major order over dy in -3..3, dx in -4..4, both non-zero, set where
 // neighbour + 1 < centre; borders replicated (lib/nx_stereo/image.ex:508-537).
-// A 32x8 block stages its window of 40x14 pixels in shared memory.
+// A tile of 32 x ROWS pixels stages its window of 40 x (ROWS + 6) pixels in
+// shared memory (`tile`, at least census_tile_bytes(ROWS)); THREADS threads
+// share the work.
 constexpr int kCensusX = 32, kCensusY = 8;
 
+__host__ __device__ constexpr int census_tile_bytes(int rows) { return (rows + 6) * (kCensusX + 8); }
+
+template <int ROWS, int THREADS>
 __device__ __forceinline__ void census_tile(const uint8_t *__restrict__ image, int width,
                                             int height, uint64_t *__restrict__ codes, int x0,
-                                            int y0) {
-    __shared__ uint8_t tile[kCensusY + 6][kCensusX + 8];
-    const int tid = threadIdx.y * kCensusX + threadIdx.x;
-    for (int i = tid; i < (kCensusY + 6) * (kCensusX + 8); i += kCensusX * kCensusY) {
-        int ty = i / (kCensusX + 8), tx = i % (kCensusX + 8);
+                                            int y0, int tid, uint8_t *tile) {
+    constexpr int PITCH = kCensusX + 8;
+    for (int i = tid; i < (ROWS + 6) * PITCH; i += THREADS) {
+        int ty = i / PITCH, tx = i % PITCH;
         int sy = min(max(y0 + ty - 3, 0), height - 1);
         int sx = min(max(x0 + tx - 4, 0), width - 1);
-        tile[ty][tx] = image[(size_t)sy * width + sx];
+        tile[i] = image[(size_t)sy * width + sx];
     }
     __syncthreads();
-    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-    if (x >= width || y >= height) return;
-    const int centre = tile[threadIdx.y + 3][threadIdx.x + 4];
-    uint64_t code = 0;
-    int bit = 0;
 #pragma unroll
-    for (int dy = -3; dy <= 3; ++dy) {
-        if (dy == 0) continue;
+    for (int i = tid; i < kCensusX * ROWS; i += THREADS) {
+        const int tx = i % kCensusX, ty = i / kCensusX;
+        const int x = x0 + tx, y = y0 + ty;
+        if (x >= width || y >= height) continue;
+        const uint8_t *centre_at = tile + (ty + 3) * PITCH + tx + 4;
+        const int centre = *centre_at;
+        uint64_t code = 0;
+        int bit = 0;
 #pragma unroll
-        for (int dx = -4; dx <= 4; ++dx) {
-            if (dx == 0) continue;
-            int n = tile[threadIdx.y + 3 + dy][threadIdx.x + 4 + dx];
-            code |= (uint64_t)(n + 1 < centre) << bit;
-            ++bit;
+        for (int dy = -3; dy <= 3; ++dy) {
+            if (dy == 0) continue;
+#pragma unroll
+            for (int dx = -4; dx <= 4; ++dx) {
+                if (dx == 0) continue;
+                int n = centre_at[dy * PITCH + dx];
+                code |= (uint64_t)(n + 1 < centre) << bit;
+                ++bit;
+            }
         }
+        codes[(size_t)y * width + x] = code;
     }
-    codes[(size_t)y * width + x] = code;
 }
 
 // ---------------------------------------------------------------- costs
@@ -72,10 +81,10 @@ __device__ __forceinline__ void costs_tile(const uint64_t *__restrict__ left_cod
     uint8_t *tile = staged + sizeof(uint64_t) * (2 * kCostPixels + D);
     const size_t row = (size_t)y * width;
     for (int i = threadIdx.x; i < kCostPixels; i += blockDim.x)
-        lefts[i] = x0 + i < width ? left_codes[row + x0 + i] : 0;
+        lefts[i] = x0 + i < width ? __ldcg(left_codes + row + x0 + i) : 0;
     for (int i = threadIdx.x; i < kCostPixels + D - 1; i += blockDim.x) {
         const int x = x0 - (D - 1) + i;
-        rights[i] = (x >= 0 && x < width) ? right_codes[row + x] : 0;
+        rights[i] = (x >= 0 && x < width) ? __ldcg(right_codes + row + x) : 0;
     }
     __syncthreads();
     const int groups = kCostPixels / 4, chunks = D / 16;
@@ -156,7 +165,7 @@ __device__ __forceinline__ uint4 pack16(const uint32_t *w) {
 // The start and length of scan line `line` of direction (dy, dx): rows run
 // along x, columns along y, and a diagonal enters from the first row it meets
 // (line < W) or from the side column it meets.
-__device__ __forceinline__ int line_start(int line, int dy, int dx, int W, int H, int *y0,
+__host__ __device__ __forceinline__ int line_start(int line, int dy, int dx, int W, int H, int *y0,
                                           int *x0) {
     if (dy == 0) {
         *y0 = line;
@@ -269,7 +278,7 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
             if (active && step < length) {
 #pragma unroll
                 for (int c = 0; c < CHUNKS; ++c)
-                    *reinterpret_cast<uint4 *>(dst + 16 * c) = pack16(r + 8 * c);
+                    __stcs(reinterpret_cast<uint4 *>(dst + 16 * c), pack16(r + 8 * c));
             }
             dst += stride;
             uint32_t lowest = __vimin3_u16x2(r[0], r[1], r[2]);
@@ -293,7 +302,7 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
 // starts on the first row it meets, at a distance j = 1..W from the side it
 // runs away from (length min(H, j)), or on a side column at row offset
 // k = 1..H-1 (length min(H - k, W)).
-__device__ __forceinline__ int ranked_line(int rank, int dy, int dx, int W, int H) {
+__host__ __device__ __forceinline__ int ranked_line(int rank, int dy, int dx, int W, int H) {
     if (dy == 0 || dx == 0) return rank;
     const int full = (W > H ? W - H : H - W) + 1;  // lines of the greatest length
     int j = 0, k = 0;                              // first-row distance, or side offset
@@ -350,14 +359,21 @@ __host__ __device__ inline int group_lanes(int disparities) {
 // lowest value more than one disparity from the winner; the f32 steps are
 // rounded one at a time in the reference's order. Two path volumes add as
 // bytes without carry (127 + 127 < 256) before widening to u16x2.
+//
+// Either `keys` receives each pixel's key (0xFFFFFFFF where rejected) for the
+// per-row check, or, with `right_map`, each accepted match goes straight into
+// the right image's map: right_map[y][x - d] = min of (key & 0xFFFF0000) |
+// (65535 - d) (lib/nx_stereo.ex:646-664). `values_of` is 128 / G rows of 256
+// values in shared memory.
 template <int G, int PATHS>  // PATHS 0: read u16 sums instead of path volumes
 __device__ __forceinline__ void select_pixels(const void *__restrict__ source, int width,
                                               int height, int disparities, size_t volume,
                                               float uniqueness, float *__restrict__ disparity,
-                                              uint32_t *__restrict__ keys, size_t block) {
-    constexpr int PIXELS = 128 / G;  // per block of 128 threads
-    __shared__ __align__(16) uint16_t values_of[PIXELS][256];
-    const int slot = threadIdx.x / G, member = threadIdx.x % G;
+                                              uint32_t *__restrict__ keys,
+                                              uint32_t *__restrict__ right_map, size_t block,
+                                              uint16_t (*values_of)[256]) {
+    constexpr int PIXELS = 128 / G;  // per 128 threads
+    const int slot = (threadIdx.x % 128) / G, member = threadIdx.x % G;
     const size_t pixel = block * PIXELS + slot;
     const bool valid = pixel < (size_t)width * height;
     const int D = disparities;
@@ -371,7 +387,7 @@ __device__ __forceinline__ void select_pixels(const void *__restrict__ source, i
         const size_t at = pixel * D + d0;
         if (PATHS == 0) {
             const uint4 *sums = reinterpret_cast<const uint4 *>(static_cast<const uint16_t *>(source) + at);
-            const uint4 a = sums[0], b = sums[1];
+            const uint4 a = __ldcg(sums), b = __ldcg(sums + 1);
             v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
             v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
         } else {
@@ -379,7 +395,7 @@ __device__ __forceinline__ void select_pixels(const void *__restrict__ source, i
             uint4 loaded[PATHS > 0 ? PATHS : 1];
 #pragma unroll
             for (int p = 0; p < PATHS; ++p)  // every volume's load in flight at once
-                loaded[p] = __ldg(reinterpret_cast<const uint4 *>(volumes + p * volume));
+                loaded[p] = __ldcs(reinterpret_cast<const uint4 *>(volumes + p * volume));
 #pragma unroll
             for (int p = 0; p < PATHS; p += 2) {
                 const uint4 a = loaded[p];
@@ -440,13 +456,37 @@ __device__ __forceinline__ void select_pixels(const void *__restrict__ source, i
     const bool refine = denominator > 0.0f && winner > 0 && winner < min(D - 1, x);
     const float value_f = refine ? fadd((float)winner, correction) : (float)winner;
     disparity[pixel] = accepted ? value_f : -1.0f;
-    keys[pixel] = accepted ? ((minimum << 16) | (uint32_t)winner) : kInvalidKey;
+    if (keys) keys[pixel] = accepted ? ((minimum << 16) | (uint32_t)winner) : kInvalidKey;
+    if (right_map && accepted && x - winner >= 0)  // a winner is at most x
+        atomicMin(right_map + (pixel - winner), (minimum << 16) | (65535u - (uint32_t)winner));
 }
 
 // ---------------------------------------------------------------- check
 // OpenCV's left-right check (lib/nx_stereo.ex:643-683), one block per row:
 // the right map is the per-row atomicMin of (key & 0xFFFF0000) | (65535 - d)
 // at x - d, so the cheapest match wins and ties go to the larger d.
+// A match survives unless both floor(d) and ceil(d) disagree: the right map
+// at x - d holds a match more than one disparity away. `right` is the row's
+// right map (shared or global memory).
+template <bool GLOBAL>  // the map in global memory, written earlier in the same launch
+__device__ __forceinline__ float consistent_value(float value, int x, int width,
+                                                  const uint32_t *right) {
+    int low = (int)floorf(value), high = (int)ceilf(value);
+    bool rejected = true;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        int d = k == 0 ? low : high;
+        int rx = x - d;
+        bool inside = rx >= 0 && rx < width;
+        const uint32_t *at = right + min(max(rx, 0), width - 1);
+        uint32_t found = GLOBAL ? __ldcg(at) : *at;
+        int right_d = 65535 - (int)(found & 0xFFFFu);
+        bool disagrees = inside && found != kInvalidKey && abs(right_d - d) > 1;
+        rejected = rejected && disagrees;
+    }
+    return (value >= 0.0f && !rejected) ? value : -1.0f;
+}
+
 // `right` is the block's shared array of `width` words.
 __device__ __forceinline__ void consistency_row(const float *__restrict__ disparity,
                                                 const uint32_t *__restrict__ keys, int width,
@@ -456,29 +496,15 @@ __device__ __forceinline__ void consistency_row(const float *__restrict__ dispar
     for (int x = threadIdx.x; x < width; x += blockDim.x) right[x] = kInvalidKey;
     __syncthreads();
     for (int x = threadIdx.x; x < width; x += blockDim.x) {
-        uint32_t key = keys[row + x];
+        uint32_t key = __ldcg(keys + row + x);
         if (key == kInvalidKey) continue;
         int winner = (int)(key & 0xFFFFu);
         if (x - winner < 0) continue;  // a winner is at most x (past-edge costs lose)
         atomicMin(&right[x - winner], (key & 0xFFFF0000u) | (65535u - (uint32_t)winner));
     }
     __syncthreads();
-    for (int x = threadIdx.x; x < width; x += blockDim.x) {
-        float value = disparity[row + x];
-        int low = (int)floorf(value), high = (int)ceilf(value);
-        bool rejected = true;
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            int d = k == 0 ? low : high;
-            int rx = x - d;
-            bool inside = rx >= 0 && rx < width;
-            uint32_t found = right[min(max(rx, 0), width - 1)];
-            int right_d = 65535 - (int)(found & 0xFFFFu);
-            bool disagrees = inside && found != kInvalidKey && abs(right_d - d) > 1;
-            rejected = rejected && disagrees;
-        }
-        checked[row + x] = (value >= 0.0f && !rejected) ? value : -1.0f;
-    }
+    for (int x = threadIdx.x; x < width; x += blockDim.x)
+        checked[row + x] = consistent_value<false>(__ldcg(disparity + row + x), x, width, right);
 }
 
 // ---------------------------------------------------------------- median
@@ -501,7 +527,7 @@ __device__ __forceinline__ void median_at(const float *__restrict__ image, int w
 #pragma unroll
         for (int dx = -1; dx <= 1; ++dx) {
             int sy = min(max(y + dy, 0), height - 1), sx = min(max(x + dx, 0), width - 1);
-            v[(dy + 1) * 3 + dx + 1] = image[(size_t)sy * width + sx];
+            v[(dy + 1) * 3 + dx + 1] = __ldcg(image + (size_t)sy * width + sx);
         }
     exchange(v[1], v[2]); exchange(v[4], v[5]); exchange(v[7], v[8]);
     exchange(v[0], v[1]); exchange(v[3], v[4]); exchange(v[6], v[7]);

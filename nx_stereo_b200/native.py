@@ -72,6 +72,23 @@ class Camera(ctypes.Structure):
                 ("inverse_pr", ctypes.c_float * 9)]
 
 
+class BatchPair(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("params", SgmParams)]
+
+
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("blocks_per_sm", ctypes.c_int32), ("cost_rows", ctypes.c_int32),
+                ("select_passes", ctypes.c_int32), ("group_pairs", ctypes.c_int32),
+                ("quantum_us", ctypes.c_float), ("order", ctypes.c_int32)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("pairs", ctypes.c_uint32), ("items", ctypes.c_uint32), ("runs", ctypes.c_uint32),
+                ("blocks", ctypes.c_uint32), ("shared_bytes", ctypes.c_uint64),
+                ("device_bytes", ctypes.c_uint64), ("input_bytes", ctypes.c_uint64),
+                ("output_bytes", ctypes.c_uint64)]
+
+
 DONE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint64)
 
 _P = ctypes.c_void_p
@@ -110,6 +127,21 @@ SIGNATURES = {
     "nxs_depth_device": (_i, [_P, _u64, _f, _f, _P, _P, _P]),
     "nxs_cloud_device": (_i, [_P, _u32, _u32, _u32, _f, _f, _f, _f, _f, _P, _P, _P]),
     "nxs_quality_device": (_i, [_P, _P, _u32, _u32, _P, _P]),
+    "nxs_batch_default_tuning": (None, [ctypes.POINTER(BatchTuning)]),
+    "nxs_batch_create": (_i, [_P, _u32, ctypes.POINTER(BatchPair), ctypes.POINTER(BatchTuning),
+                              ctypes.POINTER(_P)] + _err),
+    "nxs_batch_buffers": (_i, [_P, _u32, ctypes.c_int32, ctypes.POINTER(_P), ctypes.POINTER(_P),
+                               ctypes.POINTER(_P)]),
+    "nxs_batch_retune": (_i, [_P, ctypes.POINTER(BatchTuning)] + _err),
+    "nxs_batch_run": (_i, [_P] + _err),
+    "nxs_batch_launch": (_i, [_P, ctypes.c_int32, _P] + _err),
+    "nxs_batch_check": (_i, [_P] + _err),
+    "nxs_batch_info": (_i, [_P, ctypes.POINTER(BatchStats)]),
+    "nxs_batch_clocks": (_i, [_P, ctypes.POINTER(_u64)]),
+    "nxs_batch_queue": (_i, [_u32, ctypes.POINTER(BatchPair), ctypes.POINTER(BatchTuning),
+                             ctypes.POINTER(_u32), ctypes.POINTER(_u32), _u32,
+                             ctypes.POINTER(_u32)] + _err),
+    "nxs_batch_destroy": (None, [_P]),
 }
 
 _lib = None
