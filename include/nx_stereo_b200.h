@@ -184,6 +184,13 @@ typedef struct {
 nxs_status nxs_sgm_check(const nxs_sgm_params *params, uint32_t width, uint32_t height,
                          char *error, size_t error_len);
 
+/* The shape of the path-aggregation kernels at `disparities` disparities:
+ * each lane of a scan line holds `words` u16x2 words (4, 8 or 16, so 8, 16
+ * or 32 disparities). A tuning knob for the whole library (nx_stereo_b200.batch's
+ * autotuner sets it); results do not depend on it. */
+nxs_status nxs_set_path_words(uint32_t disparities, uint32_t words);
+uint32_t nxs_path_words(uint32_t disparities);
+
 /* The disparity of each left pixel, -1.0 where unmatched: NxStereo.sgm/3 on a
  * rectified u8 pair in host memory (lib/nx_stereo.ex:64-74; natively
  * Matcher::disparity, native/stereo_match/src/lib.rs:105-124). Synchronous. */
@@ -337,6 +344,7 @@ typedef struct {
     int32_t group_pairs;    /* pairs a group of the queue's pipeline holds, 1..1024 */
     float quantum_us;       /* whole-GPU microseconds of one run of a phase in the queue */
     int32_t order;          /* 0: the group pipeline; 1: each phase over all pairs in turn */
+    int32_t path_words;     /* u16x2 words a path lane holds, 4, 8 or 16; 0: nxs_path_words */
 } nxs_batch_tuning;
 
 typedef struct {

@@ -22,7 +22,7 @@ from . import native
 
 PHASES = ("census", "costs", "paths", "select", "check", "median")
 TUNING_FIELDS = ("blocks_per_sm", "cost_rows", "select_passes", "group_pairs", "quantum_us",
-                 "order")
+                 "order", "path_words")
 
 
 def default_tuning():
@@ -40,7 +40,8 @@ def _tuning_struct(tuning):
         merged.update(tuning)
     return native.BatchTuning(int(merged["blocks_per_sm"]), int(merged["cost_rows"]),
                               int(merged["select_passes"]), int(merged["group_pairs"]),
-                              float(merged["quantum_us"]), int(merged["order"]))
+                              float(merged["quantum_us"]), int(merged["order"]),
+                              int(merged["path_words"]))
 
 
 def _pairs_struct(shapes):
@@ -218,6 +219,7 @@ class BatchPlan:
 # The autotuner's search space: one coordinate at a time from the current
 # best, for `sweeps` sweeps.
 SEARCH = {
+    "path_words": (8, 16),
     "order": (0, 1),
     "group_pairs": (2, 4, 8, 16),
     "blocks_per_sm": (6, 8),

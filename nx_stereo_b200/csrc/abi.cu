@@ -289,6 +289,17 @@ extern "C" nxs_status nxs_sgm_check(const nxs_sgm_params *p, uint32_t width, uin
     return NXS_OK;
 }
 
+extern "C" nxs_status nxs_set_path_words(uint32_t disparities, uint32_t words) {
+    if (!supported_disparities(disparities) || (words != 4 && words != 8 && words != 16))
+        return NXS_BAD_ARGUMENT;
+    set_path_words((int)disparities, (int)words);
+    return NXS_OK;
+}
+
+extern "C" uint32_t nxs_path_words(uint32_t disparities) {
+    return (uint32_t)path_words((int)disparities);
+}
+
 extern "C" uint64_t nxs_sgm_scratch_bytes(uint32_t width, uint32_t height, uint32_t disparities) {
     return matcher_scratch_bytes((int)width, (int)height, (int)disparities);
 }

@@ -5,6 +5,9 @@
 // phases per pair: census, costs, path aggregation, selection (which also
 // builds the right image's map for the left-right check), the check, and the
 // median with Stage.Disparity's mask (lib/nx_stereo/stage/disparity.ex:162).
+// The costs and path volumes are in the permuted order of the path lanes'
+// span (span_disparity in nxs_matcher.cuh), as the single-pair matcher keeps
+// them.
 // Each phase is cut into items a block of 128 threads does: a census tile, a
 // few rows of costs, four warps of scan lines, a run of pixels to select, a
 // run of pixels to check or filter. Blocks stay resident for the whole launch
@@ -66,6 +69,7 @@ struct BatchPair {
     int stage_mask;
     int select_lanes;     // lanes per pixel in selection
     int path_lanes;       // lanes per scan line
+    int path_words;       // u16x2 words a path lane holds (4 or 8); the order's span is twice
     int census_columns;   // census tiles per row band
     int census_tiles;     // census tiles per image
     int cost_columns;     // 64-pixel blocks per row
@@ -87,14 +91,20 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-template <int G>
+// The permuted order's span: 8 with 4 words a lane, 16 otherwise.
+template <int WORDS>
+constexpr int kSpan = WORDS == 4 ? 8 : 16;
+
+template <int G, int WORDS>
 __device__ __forceinline__ void paths_item(const BatchPair &P, const PathSetup &s, int warp,
-                                           int lane, uint4 *ring) {
-    if (P.setup.disparities == 16 * G) path_warp<G, true>(P.costs, P.paths, s, warp, lane, ring);
-    else path_warp<G, false>(P.costs, P.paths, s, warp, lane, ring);
+                                           int lane, uint8_t *ring) {
+    if (P.setup.disparities == G * 2 * WORDS)
+        path_warp<G, WORDS, true, kSpan<WORDS>>(P.costs, P.paths, s, warp, lane, ring);
+    else
+        path_warp<G, WORDS, false, kSpan<WORDS>>(P.costs, P.paths, s, warp, lane, ring);
 }
 
-template <int G, int PATHS>
+template <int G, int PATHS, int SPAN>
 __device__ __forceinline__ void select_item(const BatchPair &P, int item, uint8_t *smem) {
     constexpr int PIXELS = 128 / G;
     const int W = P.setup.width, H = P.setup.height;
@@ -102,18 +112,24 @@ __device__ __forceinline__ void select_item(const BatchPair &P, int item, uint8_
     for (int pass = 0; pass < P.select_passes; ++pass) {
         const size_t block = (size_t)item * P.select_passes + pass;
         if (block * PIXELS >= pixels) break;  // the same for the whole block
-        select_pixels<G, PATHS>(P.paths, W, H, P.setup.disparities, P.setup.volume,
+        select_pixels<G, PATHS, SPAN>(P.paths, W, H, P.setup.disparities, P.setup.volume,
                                 P.uniqueness, P.raw, nullptr, P.right_map, block,
                                 reinterpret_cast<uint16_t(*)[256]>(smem));
         __syncwarp();
     }
 }
 
+template <int PATHS, int SPAN>
+__device__ __forceinline__ void select_lanes(const BatchPair &P, int item, uint8_t *smem) {
+    if (P.select_lanes == 4) select_item<4, PATHS, SPAN>(P, item, smem);
+    else if (P.select_lanes == 8) select_item<8, PATHS, SPAN>(P, item, smem);
+    else select_item<16, PATHS, SPAN>(P, item, smem);
+}
+
 template <int PATHS>
 __device__ __forceinline__ void select_dispatch(const BatchPair &P, int item, uint8_t *smem) {
-    if (P.select_lanes == 4) select_item<4, PATHS>(P, item, smem);
-    else if (P.select_lanes == 8) select_item<8, PATHS>(P, item, smem);
-    else select_item<16, PATHS>(P, item, smem);
+    if (P.path_words == 4) select_lanes<PATHS, 8>(P, item, smem);
+    else select_lanes<PATHS, 16>(P, item, smem);
 }
 
 // Waits (thread 0, or lane 0 of a warp) until `*counter` reaches `need`; gives
@@ -135,7 +151,9 @@ __device__ __forceinline__ void wait_for(const unsigned *counter, unsigned need,
 
 // A block takes items from the queue in order; an item of phase k waits for
 // every item of phase k - 1 of its pair.
-// queue[q] = (pair << 4 | phase, item) of queue position q.
+// queue[q] = (pair << 4 | phase, item) of queue position q. WIDE: with the
+// path kernels of 16 words a lane (more registers a thread).
+template <bool WIDE>
 __device__ __forceinline__ void work(const BatchPair *__restrict__ pairs,
                                      const uint2 *__restrict__ queue, unsigned total,
                                      unsigned *control, uint8_t *smem, PathSetup &setup,
@@ -194,8 +212,12 @@ __device__ __forceinline__ void work(const BatchPair *__restrict__ pairs,
             for (int r = 0; r < P.cost_rows; ++r) {
                 if (y0 + r >= H) break;  // the same for the whole block
                 if (r) __syncthreads();  // the last row's tile is read out
-                costs_tile(P.left_codes, P.right_codes, W, P.setup.disparities, P.costs, x0,
-                           y0 + r, smem);
+                if (P.path_words == 4)
+                    costs_tile<8>(P.left_codes, P.right_codes, W, P.setup.disparities, P.costs,
+                                  x0, y0 + r, smem);
+                else
+                    costs_tile<16>(P.left_codes, P.right_codes, W, P.setup.disparities, P.costs,
+                                   x0, y0 + r, smem);
             }
             break;
         }
@@ -204,11 +226,24 @@ __device__ __forceinline__ void work(const BatchPair *__restrict__ pairs,
                 reinterpret_cast<int *>(&setup)[tid] = reinterpret_cast<const int *>(&P.setup)[tid];
             __syncthreads();
             const int index = item * (kThreads / 32) + warp;
-            uint4 *ring = reinterpret_cast<uint4 *>(smem) + warp * kPrefetch * 32 + lane;
+            // A warp's ring: kPrefetch x 32 lanes x 2 x words bytes, in pieces of
+            // at most 16 bytes strided by 32 lanes; a lane starts at its piece.
+            const int bytes = 2 * P.path_words, piece = bytes < 16 ? bytes : 16;
+            uint8_t *ring = smem + warp * kPrefetch * 32 * bytes + lane * piece;
             if (index < setup.first_warp[8]) {
-                if (P.path_lanes == 4) paths_item<4>(P, setup, index, lane, ring);
-                else if (P.path_lanes == 8) paths_item<8>(P, setup, index, lane, ring);
-                else paths_item<16>(P, setup, index, lane, ring);
+                if (WIDE && P.path_words == 16) {
+                    if (P.path_lanes == 2) paths_item<2, 16>(P, setup, index, lane, ring);
+                    else if (P.path_lanes == 4) paths_item<4, 16>(P, setup, index, lane, ring);
+                    else paths_item<8, 16>(P, setup, index, lane, ring);
+                } else if (P.path_words == 8) {
+                    if (P.path_lanes == 4) paths_item<4, 8>(P, setup, index, lane, ring);
+                    else if (P.path_lanes == 8) paths_item<8, 8>(P, setup, index, lane, ring);
+                    else paths_item<16, 8>(P, setup, index, lane, ring);
+                } else {
+                    if (P.path_lanes == 8) paths_item<8, 4>(P, setup, index, lane, ring);
+                    else if (P.path_lanes == 16) paths_item<16, 4>(P, setup, index, lane, ring);
+                    else paths_item<32, 4>(P, setup, index, lane, ring);
+                }
             }
             break;
         }
@@ -247,7 +282,8 @@ __device__ __forceinline__ void work(const BatchPair *__restrict__ pairs,
     }
 }
 
-__global__ void __launch_bounds__(kThreads, 8)
+template <bool WIDE>
+__global__ void __launch_bounds__(kThreads, WIDE ? 6 : 8)
     batch_kernel(const BatchPair *__restrict__ pairs, const uint2 *__restrict__ queue,
                  unsigned total, unsigned *control) {
     extern __shared__ __align__(16) uint8_t smem[];
@@ -255,7 +291,7 @@ __global__ void __launch_bounds__(kThreads, 8)
     __shared__ unsigned long long clocks[kClocks];  // this block's cycle sums (thread 0)
     if (threadIdx.x < kClocks) clocks[threadIdx.x] = 0;
     __syncthreads();
-    work(pairs, queue, total, control, smem, setup, clocks);
+    work<WIDE>(pairs, queue, total, control, smem, setup, clocks);
     __syncthreads();
     if (threadIdx.x < kClocks)
         atomicAdd(reinterpret_cast<unsigned long long *>(control + 4) + threadIdx.x,
@@ -312,6 +348,7 @@ struct nxs_batch {
     unsigned total = 0;  // items in the queue
     int runs = 0;
     int grid = 0;
+    bool wide = false;  // some pair's path lanes hold 16 words
     size_t shared_bytes = 0;
     size_t arena_bytes = 0, input_bytes = 0, output_bytes = 0, control_bytes = 0;
     uint8_t *arena = nullptr;    // inputs | control + outputs | everything else
@@ -334,14 +371,15 @@ void shape_pair(const nxs_batch_pair &s, const nxs_batch_tuning &t, BatchPair *o
     P.uniqueness = s.params.uniqueness;
     P.stage_mask = s.params.stage_mask ? 1 : 0;
     P.select_lanes = group_lanes(D);
-    P.path_lanes = group_lanes(D);
+    P.path_words = t.path_words ? t.path_words : path_words(D);
+    P.path_lanes = path_lanes(D, P.path_words);
     P.census_columns = (W + kCensusX - 1) / kCensusX;
     P.census_tiles = P.census_columns * ((H + kCensusRows - 1) / kCensusRows);
     P.cost_columns = (W + kCostPixels - 1) / kCostPixels;
     P.cost_rows = t.cost_rows;
     P.select_passes = t.select_passes;
     const int warps = path_setup(W, H, D, (int)s.params.paths, (int)s.params.p1,
-                                 (int)s.params.p2, &P.setup);
+                                 (int)s.params.p2, P.path_lanes, &P.setup);
     // The path volumes lie 256-aligned apart rather than packed.
     P.setup.volume = align256(px * D);
     P.items[kCensus] = 2 * P.census_tiles;
@@ -542,7 +580,8 @@ nxs_status capture(nxs_batch *b, bool host, cudaGraphExec_t *out, char *error, s
     if (host)
         cudaMemcpyAsync(b->arena, b->staging, b->input_bytes, cudaMemcpyHostToDevice, b->stream);
     cudaMemsetAsync(b->d_control, 0, b->control_bytes, b->stream);
-    batch_kernel<<<b->grid, kThreads, b->shared_bytes, b->stream>>>(
+    auto kernel = b->wide ? batch_kernel<true> : batch_kernel<false>;
+    kernel<<<b->grid, kThreads, b->shared_bytes, b->stream>>>(
         b->d_pairs, b->d_queue, b->total, b->d_control);
     if (host)
         cudaMemcpyAsync(b->staging + b->input_bytes, b->arena + b->input_bytes, b->output_bytes,
@@ -589,15 +628,19 @@ nxs_status prepare(nxs_batch *b, const nxs_batch_tuning &t, char *error, size_t 
     int max_disparities = 16;
     for (const auto &s : b->specs)
         max_disparities = std::max(max_disparities, (int)s.params.disparities);
+    int max_words = 4;
+    for (const auto &P : b->pairs) max_words = std::max(max_words, P.path_words);
+    b->wide = max_words == 16;
     b->shared_bytes = std::max({costs_shared_bytes(max_disparities),
-                                (size_t)(kThreads / 32) * kPrefetch * 32 * sizeof(uint4),
+                                (size_t)(kThreads / 32) * kPrefetch * 32 * 2 * max_words,
                                 (size_t)(128 / 4) * 256 * sizeof(uint16_t),
                                 (size_t)census_tile_bytes(kCensusRows)});
     int sms = 0, resident = 0;
     cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-    if (!e) e = cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    auto kernel = b->wide ? batch_kernel<true> : batch_kernel<false>;
+    if (!e) e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)b->shared_bytes);
-    if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, batch_kernel, kThreads,
+    if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel, kThreads,
                                                               b->shared_bytes);
     if (!e) {
         b->grid = sms * std::max(1, std::min(resident, t.blocks_per_sm));
@@ -637,10 +680,12 @@ nxs_status check_batch(uint32_t n_pairs, const nxs_batch_pair *specs,
     if (t.blocks_per_sm < 1 || t.blocks_per_sm > 16 || t.cost_rows < 1 || t.cost_rows > 64 ||
         t.select_passes < 1 || t.select_passes > 256 || t.group_pairs < 1 ||
         t.group_pairs > 1024 || !(t.quantum_us > 0.0f && t.quantum_us <= 1000.0f) ||
-        (t.order != 0 && t.order != 1)) {
+        (t.order != 0 && t.order != 1) ||
+        (t.path_words != 0 && t.path_words != 4 && t.path_words != 8 && t.path_words != 16)) {
         set_error(error, error_len,
                   "tuning out of range: blocks_per_sm 1..16, cost_rows 1..64, select_passes "
-                  "1..256, group_pairs 1..1024, quantum_us in (0, 1000], order 0 or 1");
+                  "1..256, group_pairs 1..1024, quantum_us in (0, 1000], order 0 or 1, "
+                  "path_words 0, 4, 8 or 16");
         return NXS_BAD_ARGUMENT;
     }
     for (uint32_t i = 0; i < n_pairs; ++i) {
@@ -665,6 +710,7 @@ extern "C" void nxs_batch_default_tuning(nxs_batch_tuning *t) {
     t->group_pairs = 16;
     t->quantum_us = 2.0f;
     t->order = 1;
+    t->path_words = 0;
 }
 
 extern "C" nxs_status nxs_batch_create(nxs_context *context, uint32_t n_pairs,

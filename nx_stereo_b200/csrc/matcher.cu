@@ -12,6 +12,8 @@
 // D = 128.
 #include <algorithm>
 
+#include <type_traits>
+
 #include "nxs_kernels.h"
 #include "nxs_matcher.cuh"
 
@@ -40,33 +42,56 @@ cudaError_t launch_census(const uint8_t *left, const uint8_t *right, int width, 
 }
 
 // ---------------------------------------------------------------- costs
+template <int SPAN>
 __global__ void __launch_bounds__(128)
     costs_kernel(const uint64_t *__restrict__ left_codes, const uint64_t *__restrict__ right_codes,
                  int width, int disparities, uint8_t *__restrict__ costs) {
     extern __shared__ __align__(16) uint8_t staged[];
-    costs_tile(left_codes, right_codes, width, disparities, costs, blockIdx.x * kCostPixels,
-               blockIdx.y, staged);
+    costs_tile<SPAN>(left_codes, right_codes, width, disparities, costs,
+                     blockIdx.x * kCostPixels, blockIdx.y, staged);
 }
 
 cudaError_t launch_costs(const uint64_t *left_codes, const uint64_t *right_codes, int width,
-                         int height, int disparities, uint8_t *costs, cudaStream_t stream) {
+                         int height, int disparities, uint8_t *costs, cudaStream_t stream,
+                         int span) {
     dim3 grid((width + kCostPixels - 1) / kCostPixels, height);
-    costs_kernel<<<grid, 128, costs_shared_bytes(disparities), stream>>>(
-        left_codes, right_codes, width, disparities, costs);
+    const size_t shared = costs_shared_bytes(disparities);
+#define NXS_COSTS(S)                                                                          \
+    costs_kernel<S><<<grid, 128, shared, stream>>>(left_codes, right_codes, width, disparities, \
+                                                   costs)
+    if (span == 16) NXS_COSTS(16);
+    else if (span == 8) NXS_COSTS(8);
+    else NXS_COSTS(0);
+#undef NXS_COSTS
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- paths
 // One warp per block, so blocks go to SMs as they free up, longest lines first.
-template <int G, bool FULL>
+template <int G, int WORDS, bool FULL, int SPAN>
 __global__ void __launch_bounds__(32)
     paths_kernel(const uint8_t *__restrict__ costs, uint8_t *__restrict__ paths_out,
                  const PathSetup s) {
-    __shared__ uint4 ring[kPrefetch][32];
-    path_warp<G, FULL>(costs, paths_out, s, blockIdx.x, threadIdx.x, &ring[0][threadIdx.x]);
+    using Piece = typename std::conditional<WORDS == 4, uint2, uint4>::type;
+    constexpr int PIECES = WORDS == 16 ? 2 : 1;
+    __shared__ Piece ring[kPrefetch * PIECES][32];
+    path_warp<G, WORDS, FULL, SPAN>(costs, paths_out, s, blockIdx.x, threadIdx.x,
+                                    &ring[0][threadIdx.x]);
 }
 
-int path_setup(int width, int height, int disparities, int paths, int p1, int p2,
+// Words a path lane holds at each disparity count (4, 8 or 16), the tunable
+// shape of the path kernels; words_slot maps 64..256 to the table.
+static int g_path_words[5] = {8, 8, 8, 8, 8};
+static int words_slot(int disparities) {
+    return disparities <= 64 ? 0 : disparities <= 96 ? 1 : disparities <= 128 ? 2
+                                   : disparities <= 192 ? 3 : 4;
+}
+int path_words(int disparities) { return g_path_words[words_slot(disparities)]; }
+void set_path_words(int disparities, int words) {
+    g_path_words[words_slot(disparities)] = words == 4 ? 4 : (words == 16 ? 16 : 8);
+}
+
+int path_setup(int width, int height, int disparities, int paths, int p1, int p2, int lanes,
                PathSetup *setup) {
     PathSetup &s = *setup;
     s = PathSetup{};
@@ -77,7 +102,7 @@ int path_setup(int width, int height, int disparities, int paths, int p1, int p2
     s.p2 = p2;
     s.paths = paths;
     s.volume = (size_t)width * height * disparities;
-    const int lines_per_warp = 32 / group_lanes(disparities);
+    const int lines_per_warp = 32 / lanes;
     // Rows, then columns, then diagonals.
     int n = 0;
     for (int pass = 0; pass < 3; ++pass) {
@@ -107,17 +132,46 @@ int path_setup(int width, int height, int disparities, int paths, int p1, int p2
     return total;
 }
 
-cudaError_t launch_paths(const uint8_t *costs, int width, int height, int disparities, int paths,
-                         int p1, int p2, uint8_t *paths_out, cudaStream_t stream) {
-    PathSetup s;
-    const int total = path_setup(width, height, disparities, paths, p1, p2, &s);
-    const int g = group_lanes(disparities);
-    const bool full = g * 16 == disparities;
-#define NXS_PATHS(G, F) paths_kernel<G, F><<<total, 32, 0, stream>>>(costs, paths_out, s)
-    if (g == 4) full ? NXS_PATHS(4, true) : NXS_PATHS(4, false);
-    else if (g == 8) full ? NXS_PATHS(8, true) : NXS_PATHS(8, false);
-    else full ? NXS_PATHS(16, true) : NXS_PATHS(16, false);
+template <int WORDS, bool PERMUTED>
+static void launch_paths_in(const uint8_t *costs, uint8_t *paths_out, const PathSetup &s,
+                            int total, int g, cudaStream_t stream) {
+    constexpr int SPAN = PERMUTED ? (WORDS == 4 ? 8 : 16) : 0;
+    const bool full = g * 2 * WORDS == s.disparities;
+#define NXS_PATHS(G, F)                                                                        \
+    paths_kernel<G, WORDS, F, SPAN><<<total, 32, 0, stream>>>(costs, paths_out, s)
+    if constexpr (WORDS == 16) {
+        if (g == 2) full ? NXS_PATHS(2, true) : NXS_PATHS(2, false);
+        else if (g == 4) full ? NXS_PATHS(4, true) : NXS_PATHS(4, false);
+        else full ? NXS_PATHS(8, true) : NXS_PATHS(8, false);
+    } else if constexpr (WORDS == 8) {
+        if (g == 4) full ? NXS_PATHS(4, true) : NXS_PATHS(4, false);
+        else if (g == 8) full ? NXS_PATHS(8, true) : NXS_PATHS(8, false);
+        else full ? NXS_PATHS(16, true) : NXS_PATHS(16, false);
+    } else {
+        if (g == 8) full ? NXS_PATHS(8, true) : NXS_PATHS(8, false);
+        else if (g == 16) full ? NXS_PATHS(16, true) : NXS_PATHS(16, false);
+        else full ? NXS_PATHS(32, true) : NXS_PATHS(32, false);
+    }
 #undef NXS_PATHS
+}
+
+cudaError_t launch_paths(const uint8_t *costs, int width, int height, int disparities, int paths,
+                         int p1, int p2, uint8_t *paths_out, cudaStream_t stream,
+                         bool permuted) {
+    const int words = path_words(disparities);
+    const int g = path_lanes(disparities, words);
+    PathSetup s;
+    const int total = path_setup(width, height, disparities, paths, p1, p2, g, &s);
+    if (words == 16) {
+        if (permuted) launch_paths_in<16, true>(costs, paths_out, s, total, g, stream);
+        else launch_paths_in<16, false>(costs, paths_out, s, total, g, stream);
+    } else if (words == 8) {
+        if (permuted) launch_paths_in<8, true>(costs, paths_out, s, total, g, stream);
+        else launch_paths_in<8, false>(costs, paths_out, s, total, g, stream);
+    } else {
+        if (permuted) launch_paths_in<4, true>(costs, paths_out, s, total, g, stream);
+        else launch_paths_in<4, false>(costs, paths_out, s, total, g, stream);
+    }
     return cudaGetLastError();
 }
 
@@ -146,17 +200,17 @@ cudaError_t launch_sum_paths(const uint8_t *paths_in, int width, int height, int
 }
 
 // ---------------------------------------------------------------- select
-template <int G, int PATHS>
+template <int G, int PATHS, int SPAN>
 __global__ void __launch_bounds__(128)
     select_kernel(const void *__restrict__ source, int width, int height, int disparities,
                   size_t volume, float uniqueness, float *__restrict__ disparity,
                   uint32_t *__restrict__ keys) {
     __shared__ __align__(16) uint16_t values_of[128 / G][256];
-    select_pixels<G, PATHS>(source, width, height, disparities, volume, uniqueness, disparity,
-                            keys, nullptr, blockIdx.x, values_of);
+    select_pixels<G, PATHS, SPAN>(source, width, height, disparities, volume, uniqueness,
+                                  disparity, keys, nullptr, blockIdx.x, values_of);
 }
 
-template <int PATHS>
+template <int PATHS, int SPAN = 0>
 static cudaError_t launch_select(const void *source, int width, int height, int disparities,
                                  float uniqueness, float *disparity, uint32_t *keys,
                                  cudaStream_t stream) {
@@ -165,8 +219,8 @@ static cudaError_t launch_select(const void *source, int width, int height, int 
     const int g = group_lanes(disparities);
     const unsigned blocks = (unsigned)((pixels + 128 / g - 1) / (128 / g));
 #define NXS_SELECT(G)                                                                         \
-    select_kernel<G, PATHS><<<blocks, 128, 0, stream>>>(source, width, height, disparities,    \
-                                                        volume, uniqueness, disparity, keys)
+    select_kernel<G, PATHS, SPAN><<<blocks, 128, 0, stream>>>(                                \
+        source, width, height, disparities, volume, uniqueness, disparity, keys)
     if (g == 4) NXS_SELECT(4);
     else if (g == 8) NXS_SELECT(8);
     else NXS_SELECT(16);
@@ -176,7 +230,15 @@ static cudaError_t launch_select(const void *source, int width, int height, int 
 
 cudaError_t launch_select_paths(const uint8_t *paths_in, int width, int height, int disparities,
                                 int paths, float uniqueness, float *disparity, uint32_t *keys,
-                                cudaStream_t stream) {
+                                cudaStream_t stream, int span) {
+#define NXS_SELECT_SPAN(S)                                                                     \
+    return paths == 8 ? launch_select<8, S>(paths_in, width, height, disparities, uniqueness,   \
+                                            disparity, keys, stream)                           \
+                      : launch_select<3, S>(paths_in, width, height, disparities, uniqueness,   \
+                                            disparity, keys, stream)
+    if (span == 16) NXS_SELECT_SPAN(16);
+    if (span == 8) NXS_SELECT_SPAN(8);
+#undef NXS_SELECT_SPAN
     return paths == 8 ? launch_select<8>(paths_in, width, height, disparities, uniqueness,
                                          disparity, keys, stream)
                       : launch_select<3>(paths_in, width, height, disparities, uniqueness,
@@ -255,13 +317,17 @@ cudaError_t run_matcher(const uint8_t *left, const uint8_t *right, int width, in
     cudaError_t e;
     if ((e = launch_census(left, right, width, height, s.left_codes, s.right_codes, stream)))
         return e;
+    // The intermediates are in the permuted order of the path lanes' span
+    // (span_disparity).
+    const int span = path_words(disparities) == 4 ? 8 : 16;
     if ((e = launch_costs(s.left_codes, s.right_codes, width, height, disparities, s.costs,
-                          stream)))
+                          stream, span)))
         return e;
-    if ((e = launch_paths(s.costs, width, height, disparities, paths, p1, p2, s.paths, stream)))
+    if ((e = launch_paths(s.costs, width, height, disparities, paths, p1, p2, s.paths, stream,
+                          true)))
         return e;
     if ((e = launch_select_paths(s.paths, width, height, disparities, paths, uniqueness,
-                                 s.selected, s.keys, stream)))
+                                 s.selected, s.keys, stream, span)))
         return e;
     if ((e = launch_consistency(s.selected, s.keys, width, height, s.checked, stream))) return e;
     return launch_median3(s.checked, width, height, stage_mask, disparity, stream);

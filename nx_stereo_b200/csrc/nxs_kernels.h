@@ -26,17 +26,22 @@ struct Camera {
 // to run one image).
 cudaError_t launch_census(const uint8_t *left, const uint8_t *right, int width, int height,
                           uint64_t *left_codes, uint64_t *right_codes, cudaStream_t stream);
+// span 8 or 16: each run of `span` disparities in the permuted order of
+// span_disparity (the matcher's internal order); 0: d0, d1, d2, ...
 cudaError_t launch_costs(const uint64_t *left_codes, const uint64_t *right_codes, int width,
-                         int height, int disparities, uint8_t *costs, cudaStream_t stream);
-// paths_out[p][y][x][d] (u8) for p < paths.
+                         int height, int disparities, uint8_t *costs, cudaStream_t stream,
+                         int span = 0);
+// paths_out[p][y][x][d] (u8) for p < paths; permuted: costs and path costs
+// in the permuted order of span 8 (path_words(disparities) 4) or 16.
 cudaError_t launch_paths(const uint8_t *costs, int width, int height, int disparities, int paths,
-                         int p1, int p2, uint8_t *paths_out, cudaStream_t stream);
+                         int p1, int p2, uint8_t *paths_out, cudaStream_t stream,
+                         bool permuted = false);
 // sums[y][x][d] = sum over paths of paths_in (u16).
 cudaError_t launch_sum_paths(const uint8_t *paths_in, int width, int height, int disparities,
                              int paths, uint16_t *sums, cudaStream_t stream);
 cudaError_t launch_select_paths(const uint8_t *paths_in, int width, int height, int disparities,
                                 int paths, float uniqueness, float *disparity, uint32_t *keys,
-                                cudaStream_t stream);
+                                cudaStream_t stream, int span = 0);
 cudaError_t launch_select_sums(const uint16_t *sums, int width, int height, int disparities,
                                float uniqueness, float *disparity, uint32_t *keys,
                                cudaStream_t stream);
@@ -85,8 +90,14 @@ cudaError_t run_matcher(const uint8_t *left, const uint8_t *right, int width, in
 // The device a context was opened on.
 int context_device(nxs_context *context);
 
-// The warp layout of one pair's path launch; returns the number of warps.
-int path_setup(int width, int height, int disparities, int paths, int p1, int p2,
+// The warp layout of one pair's path launch with `lanes` lanes a scan line;
+// returns the number of warps.
+int path_setup(int width, int height, int disparities, int paths, int p1, int p2, int lanes,
                struct PathSetup *setup);
+
+// Words (4, 8 or 16, so 8, 16 or 32 disparities) a path lane holds at this
+// many disparities, and setting it.
+int path_words(int disparities);
+void set_path_words(int disparities, int words);
 
 }  // namespace nxs

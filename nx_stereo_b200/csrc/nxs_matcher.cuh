@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <type_traits>
 
 #include "nxs_device.cuh"
 
@@ -59,18 +60,34 @@ __device__ __forceinline__ void census_tile(const uint8_t *__restrict__ image, i
 
 // ---------------------------------------------------------------- costs
 // costs[y][x][d] = popcount(left[y][x] ^ right[y][x - d]), right codes left of
-// the image zero (lib/nx_stereo.ex:528-542). A block of 128 threads covers 64
+// the image zero (lib/nx_stereo.ex:528-542). SPAN 8 or 16 stores each run of
+// SPAN disparities in the permuted order of span_disparity, the order the
+// matcher's own path and selection kernels work in. A block of 128 threads covers 64
 // pixels of a row. It stages their left codes and the D + 63 right codes they
 // reach; a thread computes 4 neighbouring pixels x 16 disparities, whose right
 // codes are 19 consecutive ones held in registers, into a shared tile, and the
 // block then writes its 64 x D bytes out contiguously with 16-byte stores.
 constexpr int kCostPixels = 64;
 
+// The permuted disparity order: within each run of SPAN disparities, bytes 2k
+// and 2k + 1 hold disparities k and k + SPAN / 2, so the u16x2 word k of a
+// path lane holding SPAN disparities holds (k, k + SPAN / 2), and the
+// neighbours of both halves at d - 1 and at d + 1 are the whole words k - 1
+// and k + 1. SPAN 0 is the natural order. span_disparity: the disparity at
+// byte j; span_position: the byte that holds disparity d.
+__host__ __device__ constexpr int span_disparity(int span, int j) {
+    return span == 0 ? j : (j / span) * span + (j % span) / 2 + (span / 2) * ((j % span) % 2);
+}
+__host__ __device__ constexpr int span_position(int span, int d) {
+    return span == 0 ? d : (d / span) * span + 2 * ((d % span) % (span / 2)) + (d % span) / (span / 2);
+}
+
 __host__ __device__ inline size_t costs_shared_bytes(int disparities) {
     return sizeof(uint64_t) * (2 * kCostPixels + disparities) +
            (size_t)kCostPixels * (disparities + 16);
 }
 
+template <int SPAN = 0>
 __device__ __forceinline__ void costs_tile(const uint64_t *__restrict__ left_codes,
                                            const uint64_t *__restrict__ right_codes, int width,
                                            int disparities, uint8_t *__restrict__ costs, int x0,
@@ -104,8 +121,10 @@ __device__ __forceinline__ void costs_tile(const uint64_t *__restrict__ left_cod
             for (int q = 0; q < 4; ++q) {
                 uint32_t w = 0;
 #pragma unroll
-                for (int b = 0; b < 4; ++b)
-                    w |= (uint32_t)__popcll(l ^ window[i - (4 * q + b) + 15]) << (8 * b);
+                for (int b = 0; b < 4; ++b) {
+                    const int k = span_disparity(SPAN, 4 * q + b);
+                    w |= (uint32_t)__popcll(l ^ window[i - k + 15]) << (8 * b);
+                }
                 words[q] = w;
             }
             *reinterpret_cast<uint4 *>(tile + (p0 + i) * pitch + d0) =
@@ -157,6 +176,17 @@ __device__ __forceinline__ void unpack16(const uint4 c, uint32_t *w) {
     w[7] = __byte_perm(c.w, 0, 0x4342);
 }
 
+__device__ __forceinline__ void unpack8(const uint2 c, uint32_t *w) {
+    w[0] = __byte_perm(c.x, 0, 0x4140);
+    w[1] = __byte_perm(c.x, 0, 0x4342);
+    w[2] = __byte_perm(c.y, 0, 0x4140);
+    w[3] = __byte_perm(c.y, 0, 0x4342);
+}
+
+__device__ __forceinline__ uint2 pack8(const uint32_t *w) {
+    return make_uint2(__byte_perm(w[0], w[1], 0x6420), __byte_perm(w[2], w[3], 0x6420));
+}
+
 __device__ __forceinline__ uint4 pack16(const uint32_t *w) {
     return make_uint4(__byte_perm(w[0], w[1], 0x6420), __byte_perm(w[2], w[3], 0x6420),
                       __byte_perm(w[4], w[5], 0x6420), __byte_perm(w[6], w[7], 0x6420));
@@ -198,27 +228,47 @@ __device__ __forceinline__ void copy16_async(void *shared, const void *global, b
                  "r"(valid ? 16 : 0)
                  : "memory");
 }
+__device__ __forceinline__ void copy8_async(void *shared, const void *global, bool valid) {
+    const unsigned address = (unsigned)__cvta_generic_to_shared(shared);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(address), "l"(global),
+                 "r"(valid ? 8 : 0)
+                 : "memory");
+}
 __device__ __forceinline__ void copy_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void copy_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// The lines of one warp: G lanes per line, WORDS u16x2 words per lane.
-// `ring` is this thread's kPrefetch x (WORDS / 8) slots of 16 bytes, strided
-// by THREADS threads.
-template <int G, int WORDS, bool FULL, int THREADS>
+// The lines of one warp: G lanes per line, WORDS (4, 8 or 16) u16x2 words,
+// so 2 x WORDS disparities, per lane. `ring` is this thread's first slot of
+// the warp's kPrefetch x THREADS slots of 2 x WORDS bytes. SPAN (8 or 16, at
+// most 2 x WORDS): costs and path costs are in the permuted order of
+// span_disparity, so within each run of SPAN disparities word k holds
+// disparities (k, k + SPAN / 2) and its neighbours at d - 1 and d + 1 are the
+// words k - 1 and k + 1, but for the first and last word of a run, whose
+// outer neighbour lies in the next run (one byte permute each); SPAN 0:
+// word k holds (2k, 2k + 1) and every neighbour is made by a byte permute.
+template <int G, int WORDS, bool FULL, int THREADS, int SPAN = 0>
 __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
                                              uint8_t *__restrict__ out, const PathSetup &s,
-                                             int p, int line, int member, uint4 *ring) {
-    constexpr int CHUNKS = WORDS / 8;  // 16-byte chunks per lane
+                                             int p, int line, int member, void *ring_base) {
+    static_assert(WORDS == 4 || WORDS == 8 || WORDS == 16, "4, 8 or 16 words a lane");
+    static_assert(SPAN == 0 || (SPAN >= 8 && SPAN <= 2 * WORDS && (2 * WORDS) % SPAN == 0),
+                  "a lane holds whole permuted runs");
+    constexpr int BYTES = 2 * WORDS;             // a lane's disparities, one byte each
+    constexpr int PIECE = BYTES < 16 ? BYTES : 16;  // bytes of one async copy
+    constexpr int PIECES = BYTES / PIECE;
+    constexpr int RUN = SPAN / 2;                // words of a permuted run
+    using Piece = typename std::conditional<PIECE == 16, uint4, uint2>::type;
+    Piece *ring = static_cast<Piece *>(ring_base);
     const int dy = s.dy[p], dx = s.dx[p];
     const int W = s.width, H = s.height, D = s.disparities;
     int y0 = 0, x0 = 0, length = 0;
     if (line < s.lines[p]) length = line_start(line, dy, dx, W, H, &y0, &x0);
-    const bool active = FULL || member * 2 * WORDS < D;
+    const bool active = FULL || member * BYTES < D;
     const ptrdiff_t stride = ((ptrdiff_t)dy * W + dx) * D;
-    const size_t at = ((size_t)y0 * W + x0) * D + member * 2 * WORDS;
+    const size_t at = ((size_t)y0 * W + x0) * D + member * BYTES;
     const uint8_t *ahead = costs + at;
     uint8_t *dst = out + (size_t)p * s.volume + at;
     const int steps = (int)__reduce_max_sync(kFullMask, (unsigned)length);
@@ -229,46 +279,67 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
     uint32_t m2 = 0, j2 = (uint32_t)s.p2 * 0x10001u;
     const uint32_t p1x2 = (uint32_t)s.p1 * 0x10001u, p2x2 = (uint32_t)s.p2 * 0x10001u;
 
+    auto fetch = [&](int slot, bool valid) {
 #pragma unroll
-    for (int i = 0; i < kPrefetch - 1; ++i) {
-        const bool valid = active && i < length;
-#pragma unroll
-        for (int c = 0; c < CHUNKS; ++c)
-            copy16_async(ring + (i * CHUNKS + c) * THREADS, valid ? ahead + 16 * c : costs, valid);
+        for (int c = 0; c < PIECES; ++c) {
+            Piece *to = ring + (slot * PIECES + c) * THREADS;
+            const uint8_t *from = valid ? ahead + PIECE * c : costs;
+            if (PIECE == 16) copy16_async(to, from, valid);
+            else copy8_async(to, from, valid);
+        }
         copy_commit();
         ahead += stride;
-    }
+    };
+#pragma unroll
+    for (int i = 0; i < kPrefetch - 1; ++i) fetch(i, active && i < length);
     for (int base = 0; base < steps; base += kPrefetch) {
 #pragma unroll
         for (int i = 0; i < kPrefetch; ++i) {
             const int step = base + i;
             if (step >= steps) break;  // uniform across the warp
-            {   // the copy of step + kPrefetch - 1 goes to the slot read last step
-                const bool valid = active && step + kPrefetch - 1 < length;
-                const int slot = (i + kPrefetch - 1) % kPrefetch;
-#pragma unroll
-                for (int c = 0; c < CHUNKS; ++c)
-                    copy16_async(ring + (slot * CHUNKS + c) * THREADS,
-                                 valid ? ahead + 16 * c : costs, valid);
-                copy_commit();
-                ahead += stride;
-            }
+            // the copy of step + kPrefetch - 1 goes to the slot read last step
+            fetch((i + kPrefetch - 1) % kPrefetch, active && step + kPrefetch - 1 < length);
             copy_wait<kPrefetch - 1>();
             uint32_t cost[WORDS];
 #pragma unroll
-            for (int c = 0; c < CHUNKS; ++c) unpack16(ring[(i * CHUNKS + c) * THREADS], cost + 8 * c);
+            for (int c = 0; c < PIECES; ++c) {
+                if constexpr (PIECE == 16) unpack16(ring[(i * PIECES + c) * THREADS], cost + 8 * c);
+                else unpack8(ring[(i * PIECES + c) * THREADS], cost + 4 * c);
+            }
             uint32_t from_left = __shfl_up_sync(kFullMask, r[WORDS - 1], 1);
             uint32_t from_right = __shfl_down_sync(kFullMask, r[0], 1);
             if (member == 0) from_left = kInf2;
             if (member == G - 1) from_right = kInf2;
-            uint32_t shifted[WORDS + 1];  // shifted[k]: the (d - 1) values of word k
-            shifted[0] = __byte_perm(from_left, r[0], 0x5432);
+            uint32_t below[WORDS], above[WORDS];  // word k's values at d - 1 and at d + 1
+            if constexpr (SPAN != 0) {
 #pragma unroll
-            for (int k = 1; k < WORDS; ++k) shifted[k] = __byte_perm(r[k - 1], r[k], 0x5432);
-            shifted[WORDS] = __byte_perm(r[WORDS - 1], from_right, 0x5432);
+                for (int k = 0; k < WORDS; ++k) {
+                    const int first = k - k % RUN, last = first + RUN - 1;
+                    if (k == first)  // (the run before's last disparity, this run's middle - 1)
+                        below[k] = __byte_perm(first ? r[first - 1] : from_left, r[last], 0x5432);
+                    else
+                        below[k] = r[k - 1];
+                    if (k == last)  // (this run's middle, the next run's first disparity)
+                        above[k] = __byte_perm(r[first], last + 1 < WORDS ? r[last + 1] : from_right,
+                                               0x5432);
+                    else
+                        above[k] = r[k + 1];
+                }
+            } else {
+                uint32_t shifted[WORDS + 1];  // shifted[k]: the (d - 1) values of word k
+                shifted[0] = __byte_perm(from_left, r[0], 0x5432);
+#pragma unroll
+                for (int k = 1; k < WORDS; ++k) shifted[k] = __byte_perm(r[k - 1], r[k], 0x5432);
+                shifted[WORDS] = __byte_perm(r[WORDS - 1], from_right, 0x5432);
+#pragma unroll
+                for (int k = 0; k < WORDS; ++k) {
+                    below[k] = shifted[k];
+                    above[k] = shifted[k + 1];
+                }
+            }
 #pragma unroll
             for (int k = 0; k < WORDS; ++k) {
-                const uint32_t neighbour = vmin2(shifted[k], shifted[k + 1]);
+                const uint32_t neighbour = vmin2(below[k], above[k]);
                 uint32_t t = vmin2(r[k], j2);
                 t = __viaddmin_u16x2(neighbour, p1x2, t);
                 // t >= m in both halves, so the subtraction borrows nowhere.
@@ -277,19 +348,23 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
             }
             if (active && step < length) {
 #pragma unroll
-                for (int c = 0; c < CHUNKS; ++c)
-                    __stcs(reinterpret_cast<uint4 *>(dst + 16 * c), pack16(r + 8 * c));
+                for (int c = 0; c < PIECES; ++c) {
+                    if constexpr (PIECE == 16)
+                        __stcs(reinterpret_cast<uint4 *>(dst + 16 * c), pack16(r + 8 * c));
+                    else
+                        __stcs(reinterpret_cast<uint2 *>(dst + 8 * c), pack8(r + 4 * c));
+                }
             }
             dst += stride;
+            // The lowest path cost over the line's disparities, in both halves.
             uint32_t lowest = __vimin3_u16x2(r[0], r[1], r[2]);
 #pragma unroll
             for (int k = 3; k + 1 < WORDS; k += 2) lowest = __vimin3_u16x2(lowest, r[k], r[k + 1]);
             if (WORDS % 2 == 0) lowest = vmin2(lowest, r[WORDS - 1]);
-            uint32_t m = min(lowest & 0xFFFFu, lowest >> 16);
 #pragma unroll
             for (int offset = G / 2; offset >= 1; offset /= 2)
-                m = min(m, __shfl_xor_sync(kFullMask, m, offset));
-            m2 = m * 0x10001u;
+                lowest = vmin2(lowest, __shfl_xor_sync(kFullMask, lowest, offset));
+            m2 = vmin2(lowest, __byte_perm(lowest, 0, 0x1032));
             j2 = m2 + p2x2;
         }
     }
@@ -323,10 +398,12 @@ __host__ __device__ __forceinline__ int ranked_line(int rank, int dy, int dx, in
 
 // One warp's lines: warp `warp` of the pair's path launch, lane `lane`.
 // Rows, then columns, then the diagonals of all four directions by rank.
-template <int G, bool FULL>
+// `ring`: this lane's first slot of the warp's kPrefetch x 32 slots of
+// 2 x WORDS bytes (in pieces of at most 16 bytes, strided by 32 lanes).
+template <int G, int WORDS, bool FULL, int SPAN = 0>
 __device__ __forceinline__ void path_warp(const uint8_t *__restrict__ costs,
                                           uint8_t *__restrict__ paths_out, const PathSetup &s,
-                                          int warp, int lane, uint4 *ring) {
+                                          int warp, int lane, void *ring) {
     int slot = 0;
     while (warp >= s.first_warp[slot + 1]) ++slot;
     int p, group;
@@ -342,13 +419,21 @@ __device__ __forceinline__ void path_warp(const uint8_t *__restrict__ costs,
     const int rank = group * (32 / G) + lane / G;
     const int line =
         rank < s.lines[p] ? ranked_line(rank, s.dy[p], s.dx[p], s.width, s.height) : rank;
-    follow_lines<G, 8, FULL, 32>(costs, paths_out, s, p, line, lane % G, ring);
+    follow_lines<G, WORDS, FULL, 32, SPAN>(costs, paths_out, s, p, line, lane % G, ring);
 }
 
-// Lanes per line (paths) or per pixel (selection), 16 disparities each: a
-// power of two.
+// Lanes per pixel (selection) or per line (paths with 16 disparities a lane),
+// 16 disparities each: a power of two.
 __host__ __device__ inline int group_lanes(int disparities) {
     return disparities <= 64 ? 4 : (disparities <= 128 ? 8 : 16);
+}
+
+// Lanes per scan line with `words` u16x2 words (2 x words disparities) a
+// lane: the power of two that covers the disparities.
+__host__ __device__ inline int path_lanes(int disparities, int words) {
+    int g = 1;
+    while (g * 2 * words < disparities) g *= 2;
+    return g;
 }
 
 // ---------------------------------------------------------------- select
@@ -365,7 +450,8 @@ __host__ __device__ inline int group_lanes(int disparities) {
 // the right image's map: right_map[y][x - d] = min of (key & 0xFFFF0000) |
 // (65535 - d) (lib/nx_stereo.ex:646-664). `values_of` is 128 / G rows of 256
 // values in shared memory.
-template <int G, int PATHS>  // PATHS 0: read u16 sums instead of path volumes
+// SPAN: the path volumes' disparity order (span_disparity).
+template <int G, int PATHS, int SPAN = 0>  // PATHS 0: u16 sums, not path volumes
 __device__ __forceinline__ void select_pixels(const void *__restrict__ source, int width,
                                               int height, int disparities, size_t volume,
                                               float uniqueness, float *__restrict__ disparity,
@@ -408,8 +494,11 @@ __device__ __forceinline__ void select_pixels(const void *__restrict__ source, i
         }
         if (x < d0 + 15) {  // disparities past the left edge lose
 #pragma unroll
-            for (int k = 0; k < 8; ++k)
-                v[k] += (d0 + 2 * k > x ? 0x8000u : 0u) | (d0 + 2 * k + 1 > x ? 0x80000000u : 0u);
+            for (int k = 0; k < 8; ++k) {
+                const int lo = d0 + span_disparity(SPAN, 2 * k);
+                const int hi = d0 + span_disparity(SPAN, 2 * k + 1);
+                v[k] += (lo > x ? 0x8000u : 0u) | (hi > x ? 0x80000000u : 0u);
+            }
         }
         *reinterpret_cast<uint4 *>(&values_of[slot][d0]) = make_uint4(v[0], v[1], v[2], v[3]);
         *reinterpret_cast<uint4 *>(&values_of[slot][d0 + 8]) = make_uint4(v[4], v[5], v[6], v[7]);
@@ -418,7 +507,9 @@ __device__ __forceinline__ void select_pixels(const void *__restrict__ source, i
     if (active) {
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const uint32_t d = (uint32_t)(d0 + 2 * k) | ((uint32_t)(d0 + 2 * k + 1) << 16);
+            const uint32_t lo = d0 + span_disparity(SPAN, 2 * k);
+            const uint32_t hi = d0 + span_disparity(SPAN, 2 * k + 1);
+            const uint32_t d = lo | (hi << 16);
             best = min(best, min(__byte_perm(v[k], d, 0x1054), __byte_perm(v[k], d, 0x3276)));
         }
     }
@@ -431,10 +522,11 @@ __device__ __forceinline__ void select_pixels(const void *__restrict__ source, i
     if (active) {
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const int d = d0 + 2 * k;
+            const int lo = d0 + span_disparity(SPAN, 2 * k);
+            const int hi = d0 + span_disparity(SPAN, 2 * k + 1);
             // d outside [winner - 1, winner + 1]
-            if ((unsigned)(d - winner + 1) > 2u) second = min(second, v[k] & 0xFFFFu);
-            if ((unsigned)(d + 1 - winner + 1) > 2u) second = min(second, v[k] >> 16);
+            if ((unsigned)(lo - winner + 1) > 2u) second = min(second, v[k] & 0xFFFFu);
+            if ((unsigned)(hi - winner + 1) > 2u) second = min(second, v[k] >> 16);
         }
     }
 #pragma unroll
@@ -442,8 +534,9 @@ __device__ __forceinline__ void select_pixels(const void *__restrict__ source, i
         second = min(second, __shfl_xor_sync(kFullMask, second, offset));
     __syncwarp();
     if (member != 0 || !valid) return;
-    const uint32_t lower = values_of[slot][max(winner - 1, 0)];
-    const uint32_t upper = values_of[slot][min(winner + 1, D - 1)];
+    const int below = max(winner - 1, 0), above = min(winner + 1, D - 1);
+    const uint32_t lower = values_of[slot][span_position(SPAN, below)];
+    const uint32_t upper = values_of[slot][span_position(SPAN, above)];
     const float lower_f = (float)lower, upper_f = (float)upper, minimum_f = (float)minimum;
     // With no disparity outside the winner's neighbours the reference's
     // minimum is i32::MAX (lib/nx_stereo.ex:620-622).

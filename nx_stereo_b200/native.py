@@ -79,7 +79,8 @@ class BatchPair(ctypes.Structure):
 class BatchTuning(ctypes.Structure):
     _fields_ = [("blocks_per_sm", ctypes.c_int32), ("cost_rows", ctypes.c_int32),
                 ("select_passes", ctypes.c_int32), ("group_pairs", ctypes.c_int32),
-                ("quantum_us", ctypes.c_float), ("order", ctypes.c_int32)]
+                ("quantum_us", ctypes.c_float), ("order", ctypes.c_int32),
+                ("path_words", ctypes.c_int32)]
 
 
 class BatchStats(ctypes.Structure):
@@ -113,6 +114,8 @@ SIGNATURES = {
     "nxs_sgm": (_i, [_P, _P, _P, _u32, _u32, ctypes.POINTER(SgmParams), _P] + _err),
     "nxs_sgm_device": (_i, [_P, _P, _P, _u32, _u32, ctypes.POINTER(SgmParams), _P, _P] + _err),
     "nxs_sgm_scratch_bytes": (_u64, [_u32, _u32, _u32]),
+    "nxs_set_path_words": (_i, [_u32, _u32]),
+    "nxs_path_words": (_u32, [_u32]),
     "nxs_census_device": (_i, [_P, _u32, _u32, _P, _P]),
     "nxs_costs_device": (_i, [_P, _P, _u32, _u32, _u32, _P, _P]),
     "nxs_aggregate_device": (_i, [_P, _P, _u32, _u32, _u32, _u32, _u32, _u32, _P, _P]),
