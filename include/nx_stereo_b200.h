@@ -157,8 +157,16 @@ nxs_status nxs_request_outputs(nxs_request *request, uint32_t *n_outputs,
 nxs_status nxs_request_times(nxs_request *request, uint32_t *n_members,
                              const uint32_t **times_us);
 
+/* When the device finished the request, in nanoseconds of CLOCK_MONOTONIC
+ * (the clock of a serving loop's arrival times); 0 while it is pending. */
+uint64_t nxs_request_done_ns(nxs_request *request);
+
 /* Frees a request; waits for it first if it is still on the device. */
 void nxs_request_free(nxs_request *request);
+
+/* The device's free and total memory in bytes, for admission control. */
+nxs_status nxs_device_memory(nxs_context *context, uint64_t *free_bytes,
+                             uint64_t *total_bytes);
 
 /* Releases segment `segment` after its requests finish. Replaces the release
  * request (protocol.rs:16). */

@@ -202,6 +202,7 @@ struct nxs_request {
     nxs_done_fn callback = nullptr;
     void *user = nullptr;
     uint64_t tag = 0;
+    std::atomic<uint64_t> done_ns{0};  // CLOCK_MONOTONIC when the device finished it
 };
 
 // ---------------------------------------------------------------------------
@@ -942,6 +943,15 @@ static void CUDART_CB request_done(void *data) {
     if (r->callback) r->callback(r->user, r->tag);
 }
 
+// Runs on the download stream before the request's done event is recorded,
+// so the event completes only after the stamp is written.
+static void CUDART_CB request_stamp(void *data) {
+    nxs_request *r = static_cast<nxs_request *>(data);
+    r->done_ns.store((uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                         std::chrono::steady_clock::now().time_since_epoch())
+                         .count());
+}
+
 extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_members,
                                     const nxs_member_params *params, uint32_t n_entries,
                                     const nxs_tensor *entries, nxs_done_fn done, void *user,
@@ -1119,6 +1129,7 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
         t.bytes = spec.bytes();
     }
     if (!e) e = cudaEventRecord(slot.free, seg->download);
+    if (!e) e = cudaLaunchHostFunc(seg->download, request_stamp, r);
     if (!e) e = cudaEventRecord(r->done, seg->download);
     if (!e && done) e = cudaLaunchHostFunc(seg->download, request_done, r);
     if (e) {
@@ -1185,6 +1196,19 @@ extern "C" nxs_status nxs_request_times(nxs_request *r, uint32_t *n_members,
     }
     *n_members = (uint32_t)r->times_us.size();
     *times_us = r->times_us.data();
+    return NXS_OK;
+}
+
+extern "C" uint64_t nxs_request_done_ns(nxs_request *r) { return r ? r->done_ns.load() : 0; }
+
+extern "C" nxs_status nxs_device_memory(nxs_context *c, uint64_t *free_bytes,
+                                        uint64_t *total_bytes) {
+    if (!c || !free_bytes || !total_bytes) return NXS_BAD_ARGUMENT;
+    cudaSetDevice(c->device);
+    size_t f = 0, t = 0;
+    if (cudaMemGetInfo(&f, &t) != cudaSuccess) return NXS_CUDA_ERROR;
+    *free_bytes = f;
+    *total_bytes = t;
     return NXS_OK;
 }
 

@@ -109,6 +109,8 @@ SIGNATURES = {
     "nxs_request_outputs": (_i, [_P, ctypes.POINTER(_u32), ctypes.POINTER(ctypes.POINTER(Tensor))]),
     "nxs_request_times": (_i, [_P, ctypes.POINTER(_u32), ctypes.POINTER(ctypes.POINTER(_u32))]),
     "nxs_request_free": (None, [_P]),
+    "nxs_request_done_ns": (_u64, [_P]),
+    "nxs_device_memory": (_i, [_P, ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
     "nxs_release": (_i, [_P, _u32]),
     "nxs_sgm_check": (_i, [ctypes.POINTER(SgmParams), _u32, _u32] + _err),
     "nxs_sgm": (_i, [_P, _P, _P, _u32, _u32, ctypes.POINTER(SgmParams), _P] + _err),
@@ -248,6 +250,10 @@ class Request:
             result[t.name.decode()] = view.copy() if copy else view
         return result
 
+    def done_ns(self):
+        """time.monotonic_ns() of the device finishing the request; 0 while pending."""
+        return int(load().nxs_request_done_ns(self._handle)) if self._handle else 0
+
     def times_us(self):
         n = ctypes.c_uint32()
         times = ctypes.POINTER(ctypes.c_uint32)()
@@ -280,6 +286,14 @@ class Context:
     @property
     def handle(self):
         return self._handle
+
+    def memory(self):
+        """(free, total) bytes of the context's device."""
+        free, total = ctypes.c_uint64(), ctypes.c_uint64()
+        status = load().nxs_device_memory(self._handle, ctypes.byref(free), ctypes.byref(total))
+        if status != OK:
+            raise NativeError(status, "device memory")
+        return free.value, total.value
 
     def close(self):
         if self._handle:

@@ -30,7 +30,10 @@ def _box3(image):
 
 
 def rectified_pair(width, height, seed=0, rectangles=6, min_disparity=4, max_disparity=56,
-                   background=(10, 20), sigma=2.0, return_disparity=False):
+                   background=(10, 20), sigma=2.0, return_disparity=False, frame=0, drift=0.0):
+    """A seeded pair (see the module's description). With drift > 0 the
+    rectangles move: each gets a speed of up to `drift` px per frame in a
+    random direction and lies where it has moved to at `frame`."""
     rng = np.random.default_rng(seed)
     left = _box3(rng.integers(0, 256, (height, width)).astype(np.float32))
     yy, xx = np.mgrid[0:height, 0:width].astype(np.float32)
@@ -52,6 +55,10 @@ def rectified_pair(width, height, seed=0, rectangles=6, min_disparity=4, max_dis
         x0, y0 = int(rng.integers(0, width - rw)), int(rng.integers(0, height - rh))
         d0 = rng.uniform(min_disparity, max_disparity)
         sx, sy = rng.uniform(-4, 4, size=2)
+        if drift > 0:
+            speed, heading = rng.uniform(0, drift), rng.uniform(0, 2 * math.pi)
+            x0 = int(np.clip(x0 + round(speed * math.cos(heading) * frame), 0, width - rw))
+            y0 = int(np.clip(y0 + round(speed * math.sin(heading) * frame), 0, height - rh))
         plane = d0 + sx * (xx[y0:y0 + rh, x0:x0 + rw] - x0) / rw \
             + sy * (yy[y0:y0 + rh, x0:x0 + rw] - y0) / rh
         region = disparity[y0:y0 + rh, x0:x0 + rw]
@@ -115,8 +122,15 @@ def _bilinear(image, x, y):
     return (1 - fy) * top + fy * bottom
 
 
-def raw_frame(rectified, side, frame_size):
-    """The raw frame whose rectification through `side` is `rectified`."""
+_maps = {}
+
+
+def _raw_map(side, frame_size):
+    """Where each raw pixel of `side` lands in the rectified image (cached)."""
+    key = (tuple(side["k"]), tuple(side["d"]), tuple(side["r"]), tuple(side["p"]),
+           tuple(frame_size))
+    if key in _maps:
+        return _maps[key]
     fh, fw = frame_size
     k = np.array(side["k"]).reshape(3, 3)
     k1, k2 = side["d"][0], side["d"][1]
@@ -131,8 +145,14 @@ def raw_frame(rectified, side, frame_size):
         x, y = xd / radial, yd / radial
     ray = np.stack([x, y, np.ones_like(x)], axis=-1) @ r.T
     pix = ray @ p3.T
-    return np.clip(np.rint(_bilinear(rectified, pix[..., 0] / pix[..., 2],
-                                     pix[..., 1] / pix[..., 2])), 0, 255).astype(np.uint8)
+    _maps[key] = (pix[..., 0] / pix[..., 2], pix[..., 1] / pix[..., 2])
+    return _maps[key]
+
+
+def raw_frame(rectified, side, frame_size):
+    """The raw frame whose rectification through `side` is `rectified`."""
+    mx, my = _raw_map(side, frame_size)
+    return np.clip(np.rint(_bilinear(rectified, mx, my)), 0, 255).astype(np.uint8)
 
 
 def raw_frames(left, right, the_rig, frame_size=None):
