@@ -11,6 +11,12 @@ host<->device copies included, up to depth() pairs in flight. Multi-GPU runs
 are independent replicas (pairs do not shard: SGM paths cross the whole
 image), timed as the max over ranks.
 
+Beside the headline, rank 0 of a one-GPU run also reports `batched` (64
+rectified pairs of mixed sizes and disparity ranges in one persistent,
+graph-captured launch, against the single-pair matcher on the same pairs),
+`large_range` (8 pairs of 1920x1080 at 256 disparities) and `serving` (32
+camera streams with Poisson arrivals at 30 pairs/s each: p50/p99 latency).
+
 `--impl reference` times the reference's CPU formulation of the same pipeline
 (the oracle's C port of the reference's Rust matcher and stages) on all host
 threads, one pair per thread per step.
@@ -43,6 +49,9 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--inputs", type=int, default=8, help="distinct pairs cycled through")
+    p.add_argument("--no-batch", action="store_true", help="skip the batched workload")
+    p.add_argument("--no-serving", action="store_true", help="skip the serving workload")
+    p.add_argument("--no-large", action="store_true", help="skip the large-range workload")
     return p.parse_args()
 
 
@@ -327,6 +336,144 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+# ---------------------------------------------------------------- other workloads
+def _time_events(torch, stream, fn, repeats):
+    """Median ms of fn() on `stream`, by CUDA events."""
+    times = []
+    with torch.cuda.stream(stream):
+        for _ in range(repeats):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            times.append(a.elapsed_time(b))
+    return statistics.median(times)
+
+
+def _plain_and_batched(torch, ctx, shapes, pairs, tuner_search=None, repeats=5):
+    """Times the batched launch (autotuned) and the single-pair matcher one pair
+    after another on the same device-resident pairs; checks every output."""
+    from nx_stereo_b200 import batch
+
+    stream = torch.cuda.Stream()
+    handle = stream.cuda_stream
+    plan = batch.BatchPlan(ctx, shapes)
+    for i, (left, right) in enumerate(pairs):
+        plan.set_inputs(i, left, right)
+    host_outputs = plan.run()  # host buffers in, one launch, host buffers out
+    tuner = batch.Autotuner(repeats=3, sweeps=1, search=tuner_search)
+    tuning, _ = tuner.tune(plan, use_cache=False)
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            plan.launch(stream=handle)
+    batched_ms = _time_events(torch, stream, lambda: plan.launch(stream=handle), repeats)
+    plan.check()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        plan.run(copy=False)
+    e2e_s = (time.perf_counter() - t0) / 3
+    devs = [(torch.from_numpy(l).cuda(), torch.from_numpy(r).cuda()) for l, r in pairs]
+    outs = [torch.empty((h, w), dtype=torch.float32, device="cuda") for w, h, _ in shapes]
+
+    def plain():
+        for (w, h, settings), (dl, dr), out in zip(shapes, devs, outs):
+            ctx.sgm_device(dl.data_ptr(), dr.data_ptr(), w, h, out.data_ptr(), stream=handle,
+                           **settings)
+
+    with torch.cuda.stream(stream):
+        plain()
+    plain_ms = _time_events(torch, stream, plain, max(2, repeats // 2))
+    torch.cuda.synchronize()
+    exact = sum(int(np.array_equal(o.cpu().numpy().view(np.uint32), h.view(np.uint32)))
+                for o, h in zip(outs, host_outputs))
+    stats = plan.stats()
+    disparities = plan.disparities()
+    b_alg = sum(8 * w * h * s["disparities"] + 6 * w * h for w, h, s in shapes)
+    plan.close()
+    n = len(shapes)
+    return {"pairs": n, "batched_ms": round(batched_ms, 3),
+            "pairs_per_s": round(n / batched_ms * 1e3, 1),
+            "mdisp_s": round(disparities / batched_ms / 1e3, 1),
+            "plain_ms": round(plain_ms, 3), "plain_pairs_per_s": round(n / plain_ms * 1e3, 1),
+            "batched_over_plain": round(plain_ms / batched_ms, 3),
+            "e2e_pairs_per_s": round(n / e2e_s, 1),
+            "e2e_api": "BatchPlan.run (C ABI nxs_batch_run: one graph, host in and out)",
+            "h2d_bytes": stats["input_bytes"], "d2h_bytes": stats["output_bytes"],
+            "bit_exact_pairs": exact, "tuning": tuning, "queue_items": stats["items"],
+            "device_gb": round(stats["device_bytes"] / 1e9, 2),
+            "b_alg_gbs": round(b_alg / batched_ms / 1e6, 1), "gpu_launches_per_batch": 1}
+
+
+def bench_batched(torch, ctx):
+    """64 rectified pairs of seeded sizes {320x240 .. 1280x720} x D {64, 96,
+    128, 192}, 8 paths, in one persistent graph-captured launch."""
+    from nx_stereo_b200 import batch, scene
+
+    shapes = batch.sample_shapes(64, seed=2024)
+    pairs = [scene.rectified_pair(w, h, seed=7000 + i, max_disparity=min(56, s["disparities"] - 8))
+             for i, (w, h, s) in enumerate(shapes)]
+    out = _plain_and_batched(torch, ctx, shapes, pairs)
+    out["workload"] = ("64 pairs, sizes drawn from 320x240, 480x270, 640x480, 728x544, 1280x720, "
+                       "disparities from 64, 96, 128, 192 (seed 2024), 8 paths")
+    return out
+
+
+def bench_large(torch, ctx):
+    """8 pairs of 1920x1080 at 256 disparities, 12 rectangles at 8-240, sigma 3."""
+    from nx_stereo_b200 import scene
+
+    shapes = [(1920, 1080, {"disparities": 256})] * 8
+    pairs = [scene.rectified_pair(1920, 1080, seed=900 + i, rectangles=12, min_disparity=8,
+                                  max_disparity=240, sigma=3.0) for i in range(8)]
+    out = _plain_and_batched(torch, ctx, shapes, pairs, repeats=3,
+                             tuner_search={"order": (0, 1), "group_pairs": (1, 2)})
+    out["workload"] = "8 pairs 1920x1080, 256 disparities, 8 paths"
+    return out
+
+
+def bench_serving(seconds=3.0):
+    """32 camera streams (728x544 and 1280x720 alternating), Poisson arrivals
+    at 30 pairs/s each, Rectification -> Disparity(128) -> SpeckleFilter ->
+    TemporalFilter -> Depth -> Quality; then every stream back to back."""
+    from nx_stereo_b200 import serving
+
+    specs = serving.synthetic_streams(32, frames=8, seed=0)
+    server = serving.Server(reserve_bytes=2 << 30)
+    ids = [server.open(g) for g, _ in specs]
+    frames_of = [fr for _, fr in specs]
+    admitted = sum(server.admitted(i) for i in ids)
+    serving.warm(server, ids, frames_of)
+    arrivals = serving.poisson_arrivals(32, 30.0, seconds, seed=1)
+    st = serving.run_load(server, ids, frames_of, arrivals)
+    server.max_in_flight = 0
+    burst = serving.run_load(server, ids, frames_of, [(0.0, s) for s in range(32) for _ in range(8)])
+    used = server.used
+    # The plain form on the same pipeline and frames: one pair at a time.
+    plain_pairs = 64
+    t0 = time.monotonic_ns()
+    for k in range(plain_pairs):
+        index = k % 32
+        server.submit(ids[index], frames_of[index][k % len(frames_of[index])])
+        while server.in_flight():
+            server.poll(wait=True)
+    plain_s = (time.monotonic_ns() - t0) / 1e9
+    for sid in ids:
+        server.close(sid)
+    return {"workload": "32 streams (16 at 728x544, 16 at 1280x720), Poisson 30 pairs/s each, "
+                        "Rect -> Disparity(128, 8 paths) -> Speckle -> Temporal -> Depth -> Quality",
+            "offered_pairs_per_s": 32 * 30, "pairs": st["pairs"],
+            "pairs_per_s": round(st["pairs_per_s"], 1), "p50_ms": round(st["p50_ms"], 3),
+            "p99_ms": round(st["p99_ms"], 3), "max_in_flight": st["max_in_flight"],
+            "streams_admitted": admitted, "device_gb_admitted": round(used / 1e9, 2),
+            "saturation_pairs_per_s": round(burst["pairs_per_s"], 1),
+            "plain_pairs_per_s": round(plain_pairs / plain_s, 1),
+            "served_over_plain": round(burst["pairs_per_s"] / (plain_pairs / plain_s), 3),
+            "latency": "arrival to device completion (CLOCK_MONOTONIC), percentile index "
+                       "ceil(n p) - 1"}
+
+
 def cpu_sample(rig, frames, threads, pairs):
     from nx_stereo_b200 import scene
     from oracle import oracle
@@ -389,6 +536,19 @@ def main():
         torch.cuda.set_device(local_rank)
         replicas.init("nccl", device=torch.device("cuda", local_rank))
     line = run_ours(args, rank, world, local_rank)
+    if rank == 0 and world == 1:
+        import torch
+
+        from nx_stereo_b200 import native
+
+        ctx = native.Context(local_rank)
+        if not args.no_batch:
+            line["batched"] = bench_batched(torch, ctx)
+        if not args.no_large:
+            line["large_range"] = bench_large(torch, ctx)
+        ctx.close()
+        if not args.no_serving:
+            line["serving"] = bench_serving()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
         rig, frames = make_inputs(4, seed=1)

@@ -92,6 +92,23 @@ struct PinnedPool {
         std::lock_guard<std::mutex> g(lock);
         free_blocks.emplace(sizes[p], p);
     }
+    // Allocates blocks of these sizes up front, so that requests do not
+    // allocate pinned memory (slow, and it can wait for the device) while
+    // pairs stream through.
+    cudaError_t reserve(const std::vector<size_t> &blocks) {
+        std::vector<void *> taken;
+        cudaError_t e = cudaSuccess;
+        for (size_t n : blocks) {
+            void *p = take(n);
+            if (!p) {
+                e = cudaErrorMemoryAllocation;
+                break;
+            }
+            taken.push_back(p);
+        }
+        for (void *p : taken) give(p);
+        return e;
+    }
     ~PinnedPool() {
         for (auto &kv : sizes) cudaFreeHost(kv.first);
     }
@@ -931,6 +948,14 @@ extern "C" nxs_status nxs_configure(nxs_context *c, uint32_t id, const nxs_geome
             e = seg->alloc(&m.missed, pixels);
             if (!e) e = cudaMemset(m.missed, 0, 4 * pixels);
         }
+    }
+    if (!e) {  // pinned staging for 2 x kSlots requests: those in flight and those read out
+        std::vector<size_t> blocks;
+        for (int k = 0; k < 2 * kSlots; ++k) {
+            for (const Spec &spec : seg->entries) blocks.push_back(spec.bytes());
+            for (const Spec &spec : seg->outputs) blocks.push_back(std::max<size_t>(spec.bytes(), 4));
+        }
+        e = seg->pinned.reserve(blocks);
     }
     if (e) return cuda_status(e, error, error_len, "segment allocation");
     std::lock_guard<std::mutex> lock(c->lock);
