@@ -165,6 +165,8 @@ class DevicePipeline:
         self.grid = torch.empty((HEIGHT // DECIMATION) * (WIDTH // DECIMATION) * 3, dtype=f32,
                                 device=dev)
         self.kept = torch.empty(1, dtype=torch.int32, device=dev)
+        # The costs and path volumes in the order the matcher itself keeps them.
+        self.span = int(native.load().nxs_matcher_span(DISPARITIES))
 
     STAGES = ["rectify", "census", "costs", "paths", "select", "consistency", "median",
               "despeckle", "depth", "cloud"]
@@ -190,14 +192,15 @@ class DevicePipeline:
         call("nxs_census_device", self.images[1].data_ptr(), WIDTH, HEIGHT,
              self.codes[1].data_ptr(), s)
         mark(2)
-        call("nxs_costs_device", self.codes[0].data_ptr(), self.codes[1].data_ptr(), WIDTH,
-             HEIGHT, DISPARITIES, self.costs.data_ptr(), s)
+        call("nxs_costs_device_ordered", self.codes[0].data_ptr(), self.codes[1].data_ptr(), WIDTH,
+             HEIGHT, DISPARITIES, self.span, self.costs.data_ptr(), s)
         mark(3)
-        call("nxs_paths_device", self.costs.data_ptr(), WIDTH, HEIGHT, DISPARITIES, PATHS, 8, 64,
-             self.volumes.data_ptr(), s)
+        call("nxs_paths_device_ordered", self.costs.data_ptr(), WIDTH, HEIGHT, DISPARITIES, PATHS,
+             8, 64, self.span, self.volumes.data_ptr(), s)
         mark(4)
-        call("nxs_select_paths_device", self.volumes.data_ptr(), WIDTH, HEIGHT, DISPARITIES,
-             PATHS, 1.0526315789473684, self.selected.data_ptr(), self.keys.data_ptr(), s)
+        call("nxs_select_paths_device_ordered", self.volumes.data_ptr(), WIDTH, HEIGHT,
+             DISPARITIES, PATHS, 1.0526315789473684, self.span, self.selected.data_ptr(),
+             self.keys.data_ptr(), s)
         mark(5)
         call("nxs_consistency_device", self.selected.data_ptr(), self.keys.data_ptr(), WIDTH,
              HEIGHT, self.checked.data_ptr(), s)

@@ -264,6 +264,25 @@ nxs_status nxs_select_paths_device(const uint8_t *d_paths, uint32_t width, uint3
                                    uint32_t disparities, uint32_t paths, float uniqueness,
                                    float *d_disparity, uint32_t *d_keys, void *stream);
 
+/* The order the matcher keeps its cost and path volumes in: within each run
+ * of `span` disparities (8 or 16), bytes 2k and 2k + 1 hold disparities k and
+ * k + span / 2, so that a packed pair of path costs has its d - 1 and d + 1
+ * neighbours in whole neighbouring words; span 0 is the natural order above.
+ * nxs_matcher_span gives the span nxs_sgm uses at this disparity count; the
+ * _ordered entry points are nxs_costs_device, nxs_paths_device and
+ * nxs_select_paths_device writing and reading their volumes in that order. */
+uint32_t nxs_matcher_span(uint32_t disparities);
+nxs_status nxs_costs_device_ordered(const uint64_t *d_left_codes, const uint64_t *d_right_codes,
+                                    uint32_t width, uint32_t height, uint32_t disparities,
+                                    uint32_t span, uint8_t *d_costs, void *stream);
+nxs_status nxs_paths_device_ordered(const uint8_t *d_costs, uint32_t width, uint32_t height,
+                                    uint32_t disparities, uint32_t paths, uint32_t p1, uint32_t p2,
+                                    uint32_t span, uint8_t *d_paths, void *stream);
+nxs_status nxs_select_paths_device_ordered(const uint8_t *d_paths, uint32_t width,
+                                           uint32_t height, uint32_t disparities, uint32_t paths,
+                                           float uniqueness, uint32_t span, float *d_disparity,
+                                           uint32_t *d_keys, void *stream);
+
 /* Winner, uniqueness and subpixel from u16 sums: f32 disparity and u32 keys
  * (lib/nx_stereo.ex:608-641). */
 nxs_status nxs_select_device(const uint16_t *d_sums, uint32_t width, uint32_t height,

@@ -330,3 +330,36 @@ def sample_shapes(count, seed, sizes=((320, 240), (480, 270), (640, 480), (728, 
         d = int(disparities[int(rng.integers(len(disparities)))])
         shapes.append((w, h, {"disparities": d, "paths": paths}))
     return shapes
+
+
+def main(argv=None):
+    """python -m nx_stereo_b200.batch [--pairs N] [--size WxH] [--disparities D]
+    [--runs R]: matches N synthetic pairs of one shape as one batch R times
+    (host buffers in and out) and prints the plan's statistics."""
+    import argparse
+
+    from . import scene
+
+    p = argparse.ArgumentParser(description=main.__doc__)
+    p.add_argument("--pairs", type=int, default=4)
+    p.add_argument("--size", default="728x544")
+    p.add_argument("--disparities", type=int, default=128)
+    p.add_argument("--runs", type=int, default=2)
+    args = p.parse_args(argv)
+    width, height = (int(v) for v in args.size.split("x"))
+    context = native.Context(0)
+    shapes = [(width, height, {"disparities": args.disparities})] * args.pairs
+    plan = BatchPlan(context, shapes)
+    for i in range(args.pairs):
+        plan.set_inputs(i, *scene.rectified_pair(width, height, seed=50 + i,
+                                                 max_disparity=min(56, args.disparities - 8)))
+    for _ in range(args.runs):
+        plan.run(copy=False)
+    print(plan.stats())
+    plan.close()
+    context.close()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -447,6 +447,50 @@ extern "C" nxs_status nxs_select_paths_device(const uint8_t *d_paths, uint32_t w
                : NXS_OK;
 }
 
+extern "C" uint32_t nxs_matcher_span(uint32_t disparities) {
+    return (uint32_t)matcher_span((int)disparities);
+}
+
+extern "C" nxs_status nxs_costs_device_ordered(const uint64_t *d_left_codes,
+                                               const uint64_t *d_right_codes, uint32_t width,
+                                               uint32_t height, uint32_t disparities,
+                                               uint32_t span, uint8_t *d_costs, void *stream) {
+    CHECK_SIZE(d_left_codes && d_right_codes && d_costs && width > 0 && height > 0 &&
+               disparities % 16 == 0 && disparities >= 16 && disparities <= 256 &&
+               (span == 0 || span == 8 || span == 16));
+    return launch_costs(d_left_codes, d_right_codes, width, height, disparities, d_costs,
+                        static_cast<cudaStream_t>(stream), (int)span)
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_paths_device_ordered(const uint8_t *d_costs, uint32_t width,
+                                               uint32_t height, uint32_t disparities,
+                                               uint32_t paths, uint32_t p1, uint32_t p2,
+                                               uint32_t span, uint8_t *d_paths, void *stream) {
+    CHECK_SIZE(d_costs && d_paths && width > 0 && height > 0 && disparities % 32 == 0 &&
+               disparities >= 32 && disparities <= 256 && (paths == 3 || paths == 8) &&
+               p1 < p2 && p2 + 48 <= 127 && (span == 0 || span == 8 || span == 16));
+    return launch_paths(d_costs, width, height, disparities, paths, p1, p2, d_paths,
+                        static_cast<cudaStream_t>(stream), (int)span)
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_select_paths_device_ordered(const uint8_t *d_paths, uint32_t width,
+                                                      uint32_t height, uint32_t disparities,
+                                                      uint32_t paths, float uniqueness,
+                                                      uint32_t span, float *d_disparity,
+                                                      uint32_t *d_keys, void *stream) {
+    CHECK_SIZE(d_paths && d_disparity && d_keys && width > 0 && height > 0 &&
+               disparities % 16 == 0 && disparities >= 16 && disparities <= 256 &&
+               (paths == 3 || paths == 8) && (span == 0 || span == 8 || span == 16));
+    return launch_select_paths(d_paths, width, height, disparities, paths, uniqueness,
+                               d_disparity, d_keys, static_cast<cudaStream_t>(stream), (int)span)
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
 extern "C" nxs_status nxs_select_device(const uint16_t *d_sums, uint32_t width, uint32_t height,
                                         uint32_t disparities, float uniqueness,
                                         float *d_disparity, uint32_t *d_keys, void *stream) {

@@ -155,10 +155,15 @@ static void launch_paths_in(const uint8_t *costs, uint8_t *paths_out, const Path
 #undef NXS_PATHS
 }
 
+int matcher_span(int disparities) { return path_words(disparities) == 4 ? 8 : 16; }
+
 cudaError_t launch_paths(const uint8_t *costs, int width, int height, int disparities, int paths,
-                         int p1, int p2, uint8_t *paths_out, cudaStream_t stream,
-                         bool permuted) {
-    const int words = path_words(disparities);
+                         int p1, int p2, uint8_t *paths_out, cudaStream_t stream, int span) {
+    // Words a lane holds: the tuned count, unless the order needs another.
+    int words = path_words(disparities);
+    if (span == 8) words = 4;
+    else if (span == 16 && words == 4) words = 8;
+    const bool permuted = span != 0;
     const int g = path_lanes(disparities, words);
     PathSetup s;
     const int total = path_setup(width, height, disparities, paths, p1, p2, g, &s);
@@ -319,12 +324,12 @@ cudaError_t run_matcher(const uint8_t *left, const uint8_t *right, int width, in
         return e;
     // The intermediates are in the permuted order of the path lanes' span
     // (span_disparity).
-    const int span = path_words(disparities) == 4 ? 8 : 16;
+    const int span = matcher_span(disparities);
     if ((e = launch_costs(s.left_codes, s.right_codes, width, height, disparities, s.costs,
                           stream, span)))
         return e;
     if ((e = launch_paths(s.costs, width, height, disparities, paths, p1, p2, s.paths, stream,
-                          true)))
+                          span)))
         return e;
     if ((e = launch_select_paths(s.paths, width, height, disparities, paths, uniqueness,
                                  s.selected, s.keys, stream, span)))

@@ -31,11 +31,13 @@ cudaError_t launch_census(const uint8_t *left, const uint8_t *right, int width, 
 cudaError_t launch_costs(const uint64_t *left_codes, const uint64_t *right_codes, int width,
                          int height, int disparities, uint8_t *costs, cudaStream_t stream,
                          int span = 0);
-// paths_out[p][y][x][d] (u8) for p < paths; permuted: costs and path costs
-// in the permuted order of span 8 (path_words(disparities) 4) or 16.
+// paths_out[p][y][x][d] (u8) for p < paths; span 8 or 16: costs and path
+// costs in that permuted order (span 0: natural).
 cudaError_t launch_paths(const uint8_t *costs, int width, int height, int disparities, int paths,
-                         int p1, int p2, uint8_t *paths_out, cudaStream_t stream,
-                         bool permuted = false);
+                         int p1, int p2, uint8_t *paths_out, cudaStream_t stream, int span = 0);
+// The order the matcher keeps its costs and path volumes in at this many
+// disparities: 8 with 4 words a path lane, 16 otherwise.
+int matcher_span(int disparities);
 // sums[y][x][d] = sum over paths of paths_in (u16).
 cudaError_t launch_sum_paths(const uint8_t *paths_in, int width, int height, int disparities,
                              int paths, uint16_t *sums, cudaStream_t stream);

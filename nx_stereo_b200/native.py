@@ -124,6 +124,10 @@ SIGNATURES = {
     "nxs_paths_device": (_i, [_P, _u32, _u32, _u32, _u32, _u32, _u32, _P, _P]),
     "nxs_select_paths_device": (_i, [_P, _u32, _u32, _u32, _u32, _f, _P, _P, _P]),
     "nxs_select_device": (_i, [_P, _u32, _u32, _u32, _f, _P, _P, _P]),
+    "nxs_matcher_span": (_u32, [_u32]),
+    "nxs_costs_device_ordered": (_i, [_P, _P, _u32, _u32, _u32, _u32, _P, _P]),
+    "nxs_paths_device_ordered": (_i, [_P, _u32, _u32, _u32, _u32, _u32, _u32, _u32, _P, _P]),
+    "nxs_select_paths_device_ordered": (_i, [_P, _u32, _u32, _u32, _u32, _f, _u32, _P, _P, _P]),
     "nxs_consistency_device": (_i, [_P, _P, _u32, _u32, _P, _P]),
     "nxs_median3_device": (_i, [_P, _u32, _u32, _u32, _P, _P]),
     "nxs_rectify_device": (_i, [_P, _u32, _u32, ctypes.POINTER(Camera), _u32, _u32, _P, _P]),
