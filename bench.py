@@ -39,6 +39,9 @@ METRIC = "pairs/s at 728x544x128 d, 8 paths (full frame-to-depth pipeline)"
 WIDTH, HEIGHT, DISPARITIES, PATHS = 728, 544, 128, 8
 DECIMATION = 4
 KERNELS_PER_STEP = 12  # rectify x2, census x2, costs, paths, select, check, median, despeckle, depth, cloud
+# DRAM bytes (read + write) of one path-aggregation launch on this workload, from
+# an ncu capture of this command (dram__bytes_read.sum + dram__bytes_write.sum).
+PATHS_TRAFFIC_BYTES = 113_165_568 + 349_915_392
 
 
 def parse():
@@ -324,7 +327,10 @@ def run_ours(args, rank, world, local_rank):
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": paths_bytes,
-                     "avg_launch_ms": round(paths_avg_s * 1000, 4), "traffic": None},
+                     "avg_launch_ms": round(paths_avg_s * 1000, 4),
+                     "traffic": PATHS_TRAFFIC_BYTES,
+                     "limiter": "integer ALU pipe (68.6% of peak issue under ncu); HBM at "
+                                "35% of peak"},
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "pipeline_roofline": {"b_alg_per_pair": b_alg,
                               "achieved_gbs": round(b_alg * value / world / 1e9, 1),
