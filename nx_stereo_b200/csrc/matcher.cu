@@ -102,6 +102,8 @@ int path_setup(int width, int height, int disparities, int paths, int p1, int p2
     s.p2 = p2;
     s.paths = paths;
     s.volume = (size_t)width * height * disparities;
+    s.one = 1u;
+    s.minus_one = 0xFFFFFFFFu;
     const int lines_per_warp = 32 / lanes;
     // Rows, then columns, then diagonals.
     int n = 0;

@@ -162,8 +162,18 @@ struct PathSetup {
     int dy[8], dx[8];
     int order[8];       // direction of each slot: rows first, then columns, then diagonals
     int straight;       // slots of rows and columns
+    // 1 and 0xFFFFFFFF, given at run time so that the recurrence's adds are
+    // issued as multiply-adds on the FMA pipe (see follow_lines).
+    unsigned one, minus_one;
     size_t volume;      // bytes of one direction's volume
 };
+
+// a * b + c (mod 2^32) as a multiply-add.
+__device__ __forceinline__ uint32_t mad_lo(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t d;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
 
 __device__ __forceinline__ void unpack16(const uint4 c, uint32_t *w) {
     w[0] = __byte_perm(c.x, 0, 0x4140);
@@ -339,11 +349,15 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
             }
 #pragma unroll
             for (int k = 0; k < WORDS; ++k) {
+                // min(prev, neighbours + p1, m + p2) - m + cost, with the adds on
+                // the FMA pipe (the min and permute work fills the integer pipe):
+                // neighbours + p1 <= 0x7FFF + 79 stays in its half; cost - m is
+                // taken mod 2^32 and t + (cost - m) equals t - m + cost, whose
+                // halves neither borrow nor carry (t >= m in both).
                 const uint32_t neighbour = vmin2(below[k], above[k]);
-                uint32_t t = vmin2(r[k], j2);
-                t = __viaddmin_u16x2(neighbour, p1x2, t);
-                // t >= m in both halves, so the subtraction borrows nowhere.
-                const uint32_t value = t - m2 + cost[k];
+                const uint32_t raised = mad_lo(neighbour, s.one, p1x2);
+                const uint32_t t = __vimin3_u16x2(r[k], j2, raised);
+                const uint32_t value = mad_lo(t, s.one, mad_lo(m2, s.minus_one, cost[k]));
                 r[k] = (FULL || active) ? value : kInf2;
             }
             if (active && step < length) {
