@@ -370,15 +370,31 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
                 }
             }
             dst += stride;
-            // The lowest path cost over the line's disparities, in both halves.
-            uint32_t lowest = __vimin3_u16x2(r[0], r[1], r[2]);
+            // The lowest path cost over the line's disparities: a shallow tree
+            // over the lane's words, both halves folded into each half, then
+            // over the line's G lanes a shuffle tree (one warp-wide reduction
+            // when the line has the whole warp; a reduction under each group's
+            // own mask measured slower than the shuffles).
+            constexpr int PARTS = (WORDS + 2) / 3;
+            uint32_t part[PARTS];
 #pragma unroll
-            for (int k = 3; k + 1 < WORDS; k += 2) lowest = __vimin3_u16x2(lowest, r[k], r[k + 1]);
-            if (WORDS % 2 == 0) lowest = vmin2(lowest, r[WORDS - 1]);
+            for (int k = 0; k < WORDS; k += 3)
+                part[k / 3] = k + 2 < WORDS ? __vimin3_u16x2(r[k], r[k + 1], r[k + 2])
+                                            : (k + 1 < WORDS ? vmin2(r[k], r[k + 1]) : r[k]);
+            uint32_t lowest = part[0];
 #pragma unroll
-            for (int offset = G / 2; offset >= 1; offset /= 2)
-                lowest = vmin2(lowest, __shfl_xor_sync(kFullMask, lowest, offset));
-            m2 = vmin2(lowest, __byte_perm(lowest, 0, 0x1032));
+            for (int k = 1; k < PARTS; k += 2)
+                lowest = k + 1 < PARTS ? __vimin3_u16x2(lowest, part[k], part[k + 1])
+                                       : vmin2(lowest, part[k]);
+            lowest = vmin2(lowest, __byte_perm(lowest, 0, 0x1032));
+            if constexpr (G == 32) {
+                m2 = __reduce_min_sync(kFullMask, lowest);
+            } else {
+#pragma unroll
+                for (int offset = G / 2; offset >= 1; offset /= 2)
+                    lowest = vmin2(lowest, __shfl_xor_sync(kFullMask, lowest, offset));
+                m2 = lowest;
+            }
             j2 = m2 + p2x2;
         }
     }
