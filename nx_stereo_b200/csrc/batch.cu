@@ -463,16 +463,17 @@ void merge(std::vector<Stream> streams, double quantum, Emit emit) {
 }
 
 // The queue. Pairs go in groups of `group_pairs`; with G0, G1, ... the
-// groups, the queue is
-//   census and costs of G0; paths of G0;
-//   then for each i: [census and costs of G(i+1) beside check and median of
-//   G(i-1)], [paths of G(i+1) beside selection of G(i)];
-//   last, check and median of the last group.
-// Each group's path items are ordered longest first over all its pairs, so
-// a group's paths end with short lines; every phase then comes at least one
-// segment after the phase it needs, and the path aggregation (integer-pipe
-// bound) runs beside selection (HBM bound). order 1 lays every phase out over
-// all pairs in turn instead.
+// groups, the queue alternates two kinds of segment, for i = -2, -1, 0, ...:
+//   A(i): census of G(i+2), costs of G(i+1), check of G(i-2), median of G(i-3);
+//   B(i): paths of G(i+1) beside the selection of G(i-1),
+// the phases of a segment interleaved in proportion to their estimated time.
+// Every phase but the paths thus comes at least a whole segment after the
+// phase it needs, so its items rarely wait; a group's costs are written just
+// before its path items read them (still in L2 for small groups); and the
+// path aggregation (integer-pipe bound) runs beside selection (HBM bound).
+// Each group's path items are ordered longest first over all its pairs, so a
+// group's paths end with short lines. order 1 lays every phase out over all
+// pairs in turn instead.
 void build_runs(const std::vector<nxs_batch_pair> &specs, const std::vector<BatchPair> &pairs,
                 const nxs_batch_tuning &tuning, std::vector<unsigned> &start,
                 std::vector<unsigned> &info, std::vector<unsigned> &first) {
@@ -509,30 +510,12 @@ void build_runs(const std::vector<nxs_batch_pair> &specs, const std::vector<Batc
         *lo = g * size;
         *hi = std::min(n, *lo + size);
     };
-    auto early = [&](int g) {  // census, then costs
+    auto one = [&](int phase, int g) {  // one phase of every pair of group g
         Stream st;
         if (g < 0 || g >= groups) return st;
         int lo, hi;
         members(g, &lo, &hi);
-        for (int phase : {(int)kCensus, (int)kCosts})
-            for (int p = lo; p < hi; ++p) st.push_back(whole(p, phase));
-        return st;
-    };
-    auto late = [&](int g) {  // check, then median
-        Stream st;
-        if (g < 0 || g >= groups) return st;
-        int lo, hi;
-        members(g, &lo, &hi);
-        for (int phase : {(int)kCheck, (int)kMedian})
-            for (int p = lo; p < hi; ++p) st.push_back(whole(p, phase));
-        return st;
-    };
-    auto selection = [&](int g) {
-        Stream st;
-        if (g < 0 || g >= groups) return st;
-        int lo, hi;
-        members(g, &lo, &hi);
-        for (int p = lo; p < hi; ++p) st.push_back(whole(p, kSelect));
+        for (int p = lo; p < hi; ++p) st.push_back(whole(p, phase));
         return st;
     };
     auto paths = [&](int g) {  // longest first over the group's pairs
@@ -563,13 +546,11 @@ void build_runs(const std::vector<nxs_batch_pair> &specs, const std::vector<Batc
         }
         return st;
     };
-    merge({early(0)}, quantum, emit);
-    merge({paths(0)}, quantum, emit);
-    for (int g = 0; g < groups; ++g) {
-        merge({early(g + 1), late(g - 1)}, quantum, emit);
-        merge({paths(g + 1), selection(g)}, quantum, emit);
+    for (int i = -2; i <= groups + 2; ++i) {
+        merge({one(kCensus, i + 2), one(kCosts, i + 1), one(kCheck, i - 2), one(kMedian, i - 3)},
+              quantum, emit);
+        merge({paths(i + 1), one(kSelect, i - 1)}, quantum, emit);
     }
-    merge({late(groups - 1)}, quantum, emit);
     start.push_back(position);
 }
 
