@@ -175,6 +175,14 @@ __device__ __forceinline__ uint32_t mad_lo(uint32_t a, uint32_t b, uint32_t c) {
     return d;
 }
 
+// p + a * b bytes for a pointer p and 32-bit a, b, as one wide multiply-add.
+template <typename T>
+__device__ __forceinline__ T *advance(T *p, int a, unsigned b) {
+    uint64_t d;
+    asm("mad.wide.s32 %0, %1, %2, %3;" : "=l"(d) : "r"(a), "r"((int)b), "l"((uint64_t)p));
+    return reinterpret_cast<T *>(d);
+}
+
 __device__ __forceinline__ void unpack16(const uint4 c, uint32_t *w) {
     w[0] = __byte_perm(c.x, 0, 0x4140);
     w[1] = __byte_perm(c.x, 0, 0x4342);
@@ -277,7 +285,8 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
     int y0 = 0, x0 = 0, length = 0;
     if (line < s.lines[p]) length = line_start(line, dy, dx, W, H, &y0, &x0);
     const bool active = FULL || member * BYTES < D;
-    const ptrdiff_t stride = ((ptrdiff_t)dy * W + dx) * D;
+    const ptrdiff_t stride = ((ptrdiff_t)dy * W + dx) * D;  // |stride| <= 4097 x 256
+    const int stride32 = (int)stride;
     const size_t at = ((size_t)y0 * W + x0) * D + member * BYTES;
     const uint8_t *ahead = costs + at;
     uint8_t *dst = out + (size_t)p * s.volume + at;
@@ -298,7 +307,7 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
             else copy8_async(to, from, valid);
         }
         copy_commit();
-        ahead += stride;
+        ahead = advance(ahead, stride32, s.one);
     };
 #pragma unroll
     for (int i = 0; i < kPrefetch - 1; ++i) fetch(i, active && i < length);
@@ -369,7 +378,7 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
                         __stcs(reinterpret_cast<uint2 *>(dst + 8 * c), pack8(r + 4 * c));
                 }
             }
-            dst += stride;
+            dst = advance(dst, stride32, s.one);
             // The lowest path cost over the line's disparities: a shallow tree
             // over the lane's words, both halves folded into each half, then
             // over the line's G lanes a shuffle tree (one warp-wide reduction
