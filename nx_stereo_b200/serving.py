@@ -120,8 +120,13 @@ class _Stream:
 class Server:
     """Admits pairs of many streams as they arrive; see the module."""
 
-    def __init__(self, device=0, reserve_bytes=2 << 30, backend=None):
+    def __init__(self, device=0, reserve_bytes=2 << 30, backend=None, max_in_flight=None):
+        """max_in_flight: at most this many pairs on the device at once, the
+        oldest arrivals first (None: every stream's slots)."""
         self.backend = backend or _Device(device)
+        self.cap = max_in_flight
+        self.ready = collections.deque()  # stream ids of waiting pairs, in arrival order
+        self._in_flight = 0
         free, _ = self.backend.memory()
         self.budget = max(0, free - reserve_bytes)
         self.used = 0
@@ -166,7 +171,7 @@ class Server:
             stream = self.pending.popleft()
             stream.segment = self.backend.open(stream.geometry, stream.stages)
             self.used += stream.need
-            self._send(stream)
+        self._pump()
 
     # -- pairs
     def submit(self, sid, entries, arrival_ns=None):
@@ -176,20 +181,34 @@ class Server:
         seq = stream.sent + len(stream.waiting) + len(stream.in_flight)
         arrival = time.monotonic_ns() if arrival_ns is None else arrival_ns
         stream.waiting.append((seq, entries, arrival))
-        self._send(stream)
+        self.ready.append(sid)
+        self._pump()
         return seq
 
-    def _send(self, stream):
-        if stream.segment is None:
+    def _pump(self):
+        """Sends waiting pairs, oldest arrival first, while the cap allows and
+        their streams are admitted and have a free slot."""
+        if not self.ready:
             return
-        while stream.waiting and len(stream.in_flight) < self.backend.depth:
+        skipped = collections.deque()
+        while self.ready and (self.cap is None or self._in_flight < self.cap):
+            sid = self.ready.popleft()
+            stream = self.streams.get(sid)
+            if stream is None:
+                continue
+            if stream.segment is None or len(stream.in_flight) >= self.backend.depth:
+                skipped.append(sid)  # its stream is busy: later arrivals may go first
+                continue
             seq, entries, arrival = stream.waiting.popleft()
             request = self.backend.send(stream.segment, entries)
             stream.in_flight.append((seq, request, arrival))
-        self.max_in_flight = max(self.max_in_flight, self.in_flight())
+            self._in_flight += 1
+        skipped.extend(self.ready)
+        self.ready = skipped
+        self.max_in_flight = max(self.max_in_flight, self._in_flight)
 
     def in_flight(self):
-        return sum(len(s.in_flight) for s in self.streams.values())
+        return self._in_flight
 
     def poll(self, wait=False):
         """The pairs finished since the last poll, oldest first per stream."""
@@ -201,7 +220,8 @@ class Server:
                     outputs, done_ns = self.backend.finish(stream.segment, request)
                     done.append(Completed(stream.id, seq, arrival, done_ns, outputs))
                     stream.sent += 1
-                self._send(stream)
+                    self._in_flight -= 1
+            self._pump()
             if done or not wait or not self.in_flight():
                 return done
             time.sleep(50e-6)

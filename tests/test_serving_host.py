@@ -116,3 +116,20 @@ def test_closing_waits_for_the_streams_pairs():
     results = server.close(a)
     assert [c.seq for c in results] == [0, 1, 2]
     assert device.closed and not server.in_flight()
+
+
+def test_a_cap_on_pairs_in_flight_sends_the_oldest_arrivals_first():
+    device = FakeDevice(free=1 << 40)
+    server = serving.Server(reserve_bytes=0, backend=device, max_in_flight=3)
+    a, b, c = (server.open(GEOMETRY) for _ in range(3))
+    order = [(a, 0), (b, 1), (a, 2), (c, 3), (b, 4), (c, 5)]
+    for k, (sid, frame) in enumerate(order):
+        server.submit(sid, {"frame": frame}, arrival_ns=k)
+    assert server.in_flight() == 3
+    assert [r["entries"]["frame"] for r in device.sent] == [0, 1, 2]
+    done = []
+    while len(done) < 6:
+        done += server.poll(wait=True)
+        assert server.in_flight() <= 3
+    assert [r["entries"]["frame"] for r in device.sent] == [0, 1, 2, 3, 4, 5]
+    assert server.max_in_flight == 3
