@@ -387,6 +387,13 @@ def _plain_and_batched(torch, ctx, shapes, pairs, tuner_search=None, repeats=5):
     for _ in range(3):
         plan.run(copy=False)
     e2e_s = (time.perf_counter() - t0) / 3
+    # The plain form end to end: nxs_sgm on each pair's host images in turn.
+    for (w, h, settings), (left, right) in zip(shapes[:2], pairs[:2]):
+        ctx.sgm(left, right, **settings)
+    t0 = time.perf_counter()
+    for (w, h, settings), (left, right) in zip(shapes, pairs):
+        ctx.sgm(left, right, **settings)
+    plain_e2e_s = time.perf_counter() - t0
     devs = [(torch.from_numpy(l).cuda(), torch.from_numpy(r).cuda()) for l, r in pairs]
     outs = [torch.empty((h, w), dtype=torch.float32, device="cuda") for w, h, _ in shapes]
 
@@ -412,6 +419,9 @@ def _plain_and_batched(torch, ctx, shapes, pairs, tuner_search=None, repeats=5):
             "plain_ms": round(plain_ms, 3), "plain_pairs_per_s": round(n / plain_ms * 1e3, 1),
             "batched_over_plain": round(plain_ms / batched_ms, 3),
             "e2e_pairs_per_s": round(n / e2e_s, 1),
+            "plain_e2e_pairs_per_s": round(n / plain_e2e_s, 1),
+            "batched_over_plain_e2e": round(plain_e2e_s / e2e_s, 3),
+            "plain_e2e_api": "nxs_sgm per pair (host images in, disparity out, synchronous)",
             "e2e_api": "BatchPlan.run (C ABI nxs_batch_run: one graph, host in and out)",
             "h2d_bytes": stats["input_bytes"], "d2h_bytes": stats["output_bytes"],
             "bit_exact_pairs": exact, "tuning": tuning, "queue_items": stats["items"],

@@ -372,6 +372,10 @@ typedef struct {
     float quantum_us;       /* whole-GPU microseconds of one run of a phase in the queue */
     int32_t order;          /* 0: the group pipeline; 1: each phase over all pairs in turn */
     int32_t path_words;     /* u16x2 words a path lane holds, 4, 8 or 16; 0: nxs_path_words */
+    int32_t engine;         /* 0: one persistent launch over the work queue; 1: each pair's
+                               single-pair kernels as a chain on one of `streams` streams,
+                               the chains overlapping (both in one CUDA graph) */
+    int32_t streams;        /* streams of engine 1, 1..64 */
 } nxs_batch_tuning;
 
 typedef struct {

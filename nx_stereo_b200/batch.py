@@ -22,7 +22,7 @@ from . import native
 
 PHASES = ("census", "costs", "paths", "select", "check", "median")
 TUNING_FIELDS = ("blocks_per_sm", "cost_rows", "select_passes", "group_pairs", "quantum_us",
-                 "order", "path_words")
+                 "order", "path_words", "engine", "streams")
 
 
 def default_tuning():
@@ -41,7 +41,8 @@ def _tuning_struct(tuning):
     return native.BatchTuning(int(merged["blocks_per_sm"]), int(merged["cost_rows"]),
                               int(merged["select_passes"]), int(merged["group_pairs"]),
                               float(merged["quantum_us"]), int(merged["order"]),
-                              int(merged["path_words"]))
+                              int(merged["path_words"]), int(merged["engine"]),
+                              int(merged["streams"]))
 
 
 def _pairs_struct(shapes):
@@ -219,6 +220,8 @@ class BatchPlan:
 # The autotuner's search space: one coordinate at a time from the current
 # best, for `sweeps` sweeps.
 SEARCH = {
+    "engine": (0, 1),
+    "streams": (4, 8, 16, 32),
     "path_words": (8, 16),
     "order": (0, 1),
     "group_pairs": (2, 4, 8, 16),

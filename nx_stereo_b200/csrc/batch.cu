@@ -358,6 +358,10 @@ struct nxs_batch {
     unsigned *d_control = nullptr;
     cudaGraphExec_t graph = nullptr;      // control reset + kernel
     cudaGraphExec_t graph_host = nullptr; // inputs in, reset, kernel, outputs out
+    // The streams engine: side streams the pairs' kernel chains fork onto.
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> joins;
+    cudaEvent_t fork = nullptr;
     std::mutex lock;
 };
 
@@ -554,6 +558,48 @@ void build_runs(const std::vector<nxs_batch_pair> &specs, const std::vector<Batc
     start.push_back(position);
 }
 
+// The streams engine: each pair's single-pair matcher (census, costs, paths,
+// selection, check, median: the kernels nxs_sgm runs) as a chain on one of
+// the side streams, forked from and joined back to the batch's stream, the
+// largest pairs first onto the least loaded stream. Chains of different pairs
+// overlap on the device: one pair's path aggregation (integer-pipe bound, with
+// few warps per SM) beside others' costs (popcount bound) and selection (HBM
+// bound).
+void fork_chains(nxs_batch *b) {
+    const int streams = (int)b->side.size();
+    cudaEventRecord(b->fork, b->stream);
+    for (cudaStream_t side : b->side) cudaStreamWaitEvent(side, b->fork, 0);
+    std::vector<int> order(b->specs.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    auto work = [&](int i) {
+        const nxs_batch_pair &s = b->specs[i];
+        return (double)s.width * s.height * s.params.disparities * s.params.paths;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work(x) > work(y); });
+    std::vector<double> load(streams, 0.0);
+    for (int i : order) {
+        const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[k] += work(i);
+        const nxs_batch_pair &s = b->specs[i];
+        const BatchPair &P = b->pairs[i];
+        MatcherScratch scratch;
+        scratch.left_codes = P.left_codes;
+        scratch.right_codes = P.right_codes;
+        scratch.costs = P.costs;
+        scratch.paths = P.paths;
+        scratch.selected = P.raw;
+        scratch.checked = P.checked;
+        scratch.keys = P.right_map;
+        run_matcher(P.left, P.right, (int)s.width, (int)s.height, (int)s.params.disparities,
+                    (int)s.params.paths, (int)s.params.p1, (int)s.params.p2, s.params.uniqueness,
+                    s.params.stage_mask ? 1 : 0, scratch, P.disparity, b->side[k]);
+    }
+    for (int k = 0; k < streams; ++k) {
+        cudaEventRecord(b->joins[k], b->side[k]);
+        cudaStreamWaitEvent(b->stream, b->joins[k], 0);
+    }
+}
+
 nxs_status capture(nxs_batch *b, bool host, cudaGraphExec_t *out, char *error, size_t error_len) {
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
@@ -561,9 +607,13 @@ nxs_status capture(nxs_batch *b, bool host, cudaGraphExec_t *out, char *error, s
     if (host)
         cudaMemcpyAsync(b->arena, b->staging, b->input_bytes, cudaMemcpyHostToDevice, b->stream);
     cudaMemsetAsync(b->d_control, 0, b->control_bytes, b->stream);
-    auto kernel = b->wide ? batch_kernel<true> : batch_kernel<false>;
-    kernel<<<b->grid, kThreads, b->shared_bytes, b->stream>>>(
-        b->d_pairs, b->d_queue, b->total, b->d_control);
+    if (b->tuning.engine == 1) {
+        fork_chains(b);
+    } else {
+        auto kernel = b->wide ? batch_kernel<true> : batch_kernel<false>;
+        kernel<<<b->grid, kThreads, b->shared_bytes, b->stream>>>(
+            b->d_pairs, b->d_queue, b->total, b->d_control);
+    }
     if (host)
         cudaMemcpyAsync(b->staging + b->input_bytes, b->arena + b->input_bytes, b->output_bytes,
                         cudaMemcpyDeviceToHost, b->stream);
@@ -627,6 +677,23 @@ nxs_status prepare(nxs_batch *b, const nxs_batch_tuning &t, char *error, size_t 
         b->grid = sms * std::max(1, std::min(resident, t.blocks_per_sm));
         b->grid = (int)std::min<size_t>((size_t)b->grid, b->total);
     }
+    if (!e && !b->fork) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    while (!e && (int)b->side.size() < t.streams) {
+        cudaStream_t side = nullptr;
+        cudaEvent_t join = nullptr;
+        e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking);
+        if (!e) e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
+        if (side) b->side.push_back(side);
+        if (join) b->joins.push_back(join);
+    }
+    if (!e && (int)b->side.size() > t.streams) {  // fewer streams than before
+        for (size_t k = t.streams; k < b->side.size(); ++k) {
+            cudaStreamDestroy(b->side[k]);
+            cudaEventDestroy(b->joins[k]);
+        }
+        b->side.resize(t.streams);
+        b->joins.resize(t.streams);
+    }
     if (b->graph) cudaGraphExecDestroy(b->graph);
     if (b->graph_host) cudaGraphExecDestroy(b->graph_host);
     b->graph = b->graph_host = nullptr;
@@ -662,11 +729,12 @@ nxs_status check_batch(uint32_t n_pairs, const nxs_batch_pair *specs,
         t.select_passes < 1 || t.select_passes > 256 || t.group_pairs < 1 ||
         t.group_pairs > 1024 || !(t.quantum_us > 0.0f && t.quantum_us <= 1000.0f) ||
         (t.order != 0 && t.order != 1) ||
-        (t.path_words != 0 && t.path_words != 4 && t.path_words != 8 && t.path_words != 16)) {
+        (t.path_words != 0 && t.path_words != 4 && t.path_words != 8 && t.path_words != 16) ||
+        (t.engine != 0 && t.engine != 1) || t.streams < 1 || t.streams > 64) {
         set_error(error, error_len,
                   "tuning out of range: blocks_per_sm 1..16, cost_rows 1..64, select_passes "
                   "1..256, group_pairs 1..1024, quantum_us in (0, 1000], order 0 or 1, "
-                  "path_words 0, 4, 8 or 16");
+                  "path_words 0, 4, 8 or 16, engine 0 or 1, streams 1..64");
         return NXS_BAD_ARGUMENT;
     }
     for (uint32_t i = 0; i < n_pairs; ++i) {
@@ -692,6 +760,8 @@ extern "C" void nxs_batch_default_tuning(nxs_batch_tuning *t) {
     t->quantum_us = 2.0f;
     t->order = 1;
     t->path_words = 0;
+    t->engine = 0;
+    t->streams = 8;
 }
 
 extern "C" nxs_status nxs_batch_create(nxs_context *context, uint32_t n_pairs,
@@ -927,6 +997,9 @@ extern "C" void nxs_batch_destroy(nxs_batch *b) {
     if (b->d_pairs) cudaFree(b->d_pairs);
     if (b->arena) cudaFree(b->arena);
     if (b->staging) cudaFreeHost(b->staging);
+    for (cudaStream_t side : b->side) cudaStreamDestroy(side);
+    for (cudaEvent_t join : b->joins) cudaEventDestroy(join);
+    if (b->fork) cudaEventDestroy(b->fork);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }

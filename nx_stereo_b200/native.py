@@ -80,7 +80,8 @@ class BatchTuning(ctypes.Structure):
     _fields_ = [("blocks_per_sm", ctypes.c_int32), ("cost_rows", ctypes.c_int32),
                 ("select_passes", ctypes.c_int32), ("group_pairs", ctypes.c_int32),
                 ("quantum_us", ctypes.c_float), ("order", ctypes.c_int32),
-                ("path_words", ctypes.c_int32)]
+                ("path_words", ctypes.c_int32), ("engine", ctypes.c_int32),
+                ("streams", ctypes.c_int32)]
 
 
 class BatchStats(ctypes.Structure):

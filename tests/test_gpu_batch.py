@@ -3,8 +3,9 @@ disparity ranges drawn as the batched workload draws them, 3 and 8 paths,
 several penalties, the stage mask on and off) comes out bit-identical to the
 single-pair matcher, which the oracle pins; runs repeat exactly, the queue
 never times out, re-tuning changes nothing in the results, the device-side
-launch agrees with the host-buffer run, and the autotuner leaves a valid,
-equally exact plan."""
+launch agrees with the host-buffer run, the engine that runs each pair's
+single-pair kernels on forked streams gives the same results, and the
+autotuner leaves a valid, equally exact plan."""
 import numpy as np
 import pytest
 
@@ -95,7 +96,9 @@ def test_retuning_changes_nothing_but_speed(ctx):
                     "group_pairs": 1},
                    {"blocks_per_sm": 6, "cost_rows": 4, "select_passes": 16, "group_pairs": 3,
                     "quantum_us": 8.0},
-                   {"order": 1}):
+                   {"order": 1},
+                   {"engine": 1, "streams": 4},
+                   {"engine": 1, "streams": 1}):
         plan.retune(**tuning)
         assert all(plan.tuning[k] == v for k, v in tuning.items())
         got = plan.run()
@@ -149,3 +152,11 @@ def test_a_batch_too_big_for_the_device_is_refused(ctx):
 
     with pytest.raises(native.NativeError, match="GB of device memory"):
         batch.BatchPlan(ctx, [(4096, 4096, {"disparities": 256})] * 16)
+
+
+def test_the_streams_engine_on_the_mixed_batch(ctx):
+    pairs = _inputs(MIXED, 600)
+    plan = _plan(ctx, MIXED, pairs, {"engine": 1, "streams": 3})
+    for (w, h, s), (left, right), got in zip(MIXED, pairs, plan.run()):
+        assert g.same_bits(got, ctx.sgm(left, right, **s)), (w, h, s)
+    plan.close()
