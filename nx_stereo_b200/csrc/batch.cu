@@ -114,7 +114,7 @@ __device__ __forceinline__ void select_item(const BatchPair &P, int item, uint8_
         if (block * PIXELS >= pixels) break;  // the same for the whole block
         select_pixels<G, PATHS, SPAN>(P.paths, W, H, P.setup.disparities, P.setup.volume,
                                 P.uniqueness, P.raw, nullptr, P.right_map, block,
-                                reinterpret_cast<uint16_t(*)[256]>(smem));
+                                reinterpret_cast<uint16_t(*)[256]>(smem), P.setup.one);
         __syncwarp();
     }
 }

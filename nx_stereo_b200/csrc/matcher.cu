@@ -207,14 +207,15 @@ cudaError_t launch_sum_paths(const uint8_t *paths_in, int width, int height, int
 }
 
 // ---------------------------------------------------------------- select
+// `one` is 1, given at run time (select_pixels adds by multiply-adds).
 template <int G, int PATHS, int SPAN>
 __global__ void __launch_bounds__(128)
     select_kernel(const void *__restrict__ source, int width, int height, int disparities,
                   size_t volume, float uniqueness, float *__restrict__ disparity,
-                  uint32_t *__restrict__ keys) {
+                  uint32_t *__restrict__ keys, uint32_t one) {
     __shared__ __align__(16) uint16_t values_of[128 / G][256];
     select_pixels<G, PATHS, SPAN>(source, width, height, disparities, volume, uniqueness,
-                                  disparity, keys, nullptr, blockIdx.x, values_of);
+                                  disparity, keys, nullptr, blockIdx.x, values_of, one);
 }
 
 template <int PATHS, int SPAN = 0>
@@ -227,7 +228,7 @@ static cudaError_t launch_select(const void *source, int width, int height, int 
     const unsigned blocks = (unsigned)((pixels + 128 / g - 1) / (128 / g));
 #define NXS_SELECT(G)                                                                         \
     select_kernel<G, PATHS, SPAN><<<blocks, 128, 0, stream>>>(                                \
-        source, width, height, disparities, volume, uniqueness, disparity, keys)
+        source, width, height, disparities, volume, uniqueness, disparity, keys, 1u)
     if (g == 4) NXS_SELECT(4);
     else if (g == 8) NXS_SELECT(8);
     else NXS_SELECT(16);

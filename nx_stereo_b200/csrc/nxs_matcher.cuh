@@ -496,7 +496,7 @@ __device__ __forceinline__ void select_pixels(const void *__restrict__ source, i
                                               float uniqueness, float *__restrict__ disparity,
                                               uint32_t *__restrict__ keys,
                                               uint32_t *__restrict__ right_map, size_t block,
-                                              uint16_t (*values_of)[256]) {
+                                              uint16_t (*values_of)[256], uint32_t one) {
     constexpr int PIXELS = 128 / G;  // per 128 threads
     const int slot = (threadIdx.x % 128) / G, member = threadIdx.x % G;
     const size_t pixel = block * PIXELS + slot;
@@ -521,14 +521,22 @@ __device__ __forceinline__ void select_pixels(const void *__restrict__ source, i
 #pragma unroll
             for (int p = 0; p < PATHS; ++p)  // every volume's load in flight at once
                 loaded[p] = __ldcs(reinterpret_cast<const uint4 *>(volumes + p * volume));
+            // The adds as multiply-adds by a run-time 1 (`one`), on the FMA pipe:
+            // the byte-wise pair sums carry nowhere (127 + 127 < 256), the u16
+            // sums neither (8 x 127 + 0x8000 < 0x10000).
 #pragma unroll
             for (int p = 0; p < PATHS; p += 2) {
                 const uint4 a = loaded[p];
-                const uint4 b = p + 1 < PATHS ? loaded[p + 1] : make_uint4(0, 0, 0, 0);
+                uint4 both = a;
+                if (p + 1 < PATHS) {
+                    const uint4 b = loaded[p + 1];
+                    both = make_uint4(mad_lo(a.x, one, b.x), mad_lo(a.y, one, b.y),
+                                      mad_lo(a.z, one, b.z), mad_lo(a.w, one, b.w));
+                }
                 uint32_t pair[8];
-                unpack16(make_uint4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w), pair);
+                unpack16(both, pair);
 #pragma unroll
-                for (int k = 0; k < 8; ++k) v[k] += pair[k];
+                for (int k = 0; k < 8; ++k) v[k] = p == 0 ? pair[k] : mad_lo(pair[k], one, v[k]);
             }
         }
         if (x < d0 + 15) {  // disparities past the left edge lose
