@@ -38,7 +38,7 @@ import numpy as np  # noqa: E402
 METRIC = "pairs/s at 728x544x128 d, 8 paths (full frame-to-depth pipeline)"
 WIDTH, HEIGHT, DISPARITIES, PATHS = 728, 544, 128, 8
 DECIMATION = 4
-KERNELS_PER_STEP = 12  # rectify x2, census x2, costs, paths, select, check, median, despeckle, depth, cloud
+KERNELS_PER_STEP = 9  # rectify, census, costs, paths, select, check+median, despeckle, depth, cloud
 # At most this many pairs on the device at once in the serving run, oldest
 # arrival first (None: up to every stream's request slots; caps of 4, 8 and 16
 # kept p99 at 30 pairs/s/stream the same and lowered the saturation rate).
@@ -175,7 +175,7 @@ class DevicePipeline:
         # The costs and path volumes in the order the matcher itself keeps them.
         self.span = int(native.load().nxs_matcher_span(DISPARITIES))
 
-    STAGES = ["rectify", "census", "costs", "paths", "select", "consistency", "median",
+    STAGES = ["rectify", "census", "costs", "paths", "select", "check_median",
               "despeckle", "depth", "cloud"]
 
     def step(self, frames, marks=None):
@@ -189,15 +189,12 @@ class DevicePipeline:
                 marks[i].record()
 
         mark(0)
-        for side in range(2):
-            call("nxs_rectify_device", frames[side].data_ptr(), WIDTH, HEIGHT,
-                 ctypes.byref(self.cameras[side]), WIDTH, HEIGHT,
-                 self.images[side].data_ptr(), s)
+        call("nxs_rectify_pair_device", frames[0].data_ptr(), frames[1].data_ptr(), WIDTH,
+             HEIGHT, ctypes.byref(self.cameras[0]), ctypes.byref(self.cameras[1]), WIDTH, HEIGHT,
+             self.images[0].data_ptr(), self.images[1].data_ptr(), s)
         mark(1)
-        call("nxs_census_device", self.images[0].data_ptr(), WIDTH, HEIGHT,
-             self.codes[0].data_ptr(), s)
-        call("nxs_census_device", self.images[1].data_ptr(), WIDTH, HEIGHT,
-             self.codes[1].data_ptr(), s)
+        call("nxs_census_pair_device", self.images[0].data_ptr(), self.images[1].data_ptr(),
+             WIDTH, HEIGHT, self.codes[0].data_ptr(), self.codes[1].data_ptr(), s)
         mark(2)
         call("nxs_costs_device_ordered", self.codes[0].data_ptr(), self.codes[1].data_ptr(), WIDTH,
              HEIGHT, DISPARITIES, self.span, self.costs.data_ptr(), s)
@@ -209,21 +206,18 @@ class DevicePipeline:
              DISPARITIES, PATHS, 1.0526315789473684, self.span, self.selected.data_ptr(),
              self.keys.data_ptr(), s)
         mark(5)
-        call("nxs_consistency_device", self.selected.data_ptr(), self.keys.data_ptr(), WIDTH,
-             HEIGHT, self.checked.data_ptr(), s)
+        call("nxs_check_median_device", self.selected.data_ptr(), self.keys.data_ptr(), WIDTH,
+             HEIGHT, 1, self.disparity.data_ptr(), s)
         mark(6)
-        call("nxs_median3_device", self.checked.data_ptr(), WIDTH, HEIGHT, 1,
-             self.disparity.data_ptr(), s)
-        mark(7)
         call("nxs_despeckle_device", self.disparity.data_ptr(), WIDTH, HEIGHT, 12.0, 1.0, 3,
              self.speckled.data_ptr(), s)
-        mark(8)
+        mark(7)
         call("nxs_depth_device", self.speckled.data_ptr(), WIDTH * HEIGHT, self.focal,
              self.baseline, self.depth_mm.data_ptr(), self.depth_m.data_ptr(), s)
-        mark(9)
+        mark(8)
         call("nxs_cloud_device", self.depth_m.data_ptr(), WIDTH, HEIGHT, DECIMATION, self.focal,
              self.cx, self.cy, 0.05, 20.0, self.grid.data_ptr(), self.kept.data_ptr(), s)
-        mark(10)
+        mark(9)
 
 
 def run_ours(args, rank, world, local_rank):

@@ -238,6 +238,11 @@ uint64_t nxs_sgm_scratch_bytes(uint32_t width, uint32_t height, uint32_t dispari
 nxs_status nxs_census_device(const uint8_t *d_image, uint32_t width, uint32_t height,
                              uint64_t *d_codes, void *stream);
 
+/* Both images' census codes in one launch. */
+nxs_status nxs_census_pair_device(const uint8_t *d_left, const uint8_t *d_right, uint32_t width,
+                                  uint32_t height, uint64_t *d_left_codes,
+                                  uint64_t *d_right_codes, void *stream);
+
 /* u8 Hamming costs, [height][width][disparities] (lib/nx_stereo.ex:528-542). */
 nxs_status nxs_costs_device(const uint64_t *d_left_codes, const uint64_t *d_right_codes,
                             uint32_t width, uint32_t height, uint32_t disparities,
@@ -299,6 +304,12 @@ nxs_status nxs_consistency_device(const float *d_disparity, const uint32_t *d_ke
 nxs_status nxs_median3_device(const float *d_image, uint32_t width, uint32_t height,
                               uint32_t stage_mask, float *d_filtered, void *stream);
 
+/* nxs_consistency_device followed by nxs_median3_device in one pass, as the
+ * matcher runs them (width at most 4096). */
+nxs_status nxs_check_median_device(const float *d_disparity, const uint32_t *d_keys,
+                                   uint32_t width, uint32_t height, uint32_t stage_mask,
+                                   float *d_filtered, void *stream);
+
 /* --- the stages around the matcher (device buffers) --- */
 
 /* A camera as NxStereo.Rectify.camera/4 builds it, rows moved by the stage
@@ -317,6 +328,14 @@ typedef struct {
 nxs_status nxs_rectify_device(const uint8_t *d_frame, uint32_t frame_width,
                               uint32_t frame_height, const nxs_camera *camera, uint32_t width,
                               uint32_t height, uint8_t *d_rectified, void *stream);
+
+/* Both frames of a pair, each through its own camera, in one launch
+ * (Stage.Rectification's step, lib/nx_stereo/stage/rectification.ex:48-58). */
+nxs_status nxs_rectify_pair_device(const uint8_t *d_left_frame, const uint8_t *d_right_frame,
+                                   uint32_t frame_width, uint32_t frame_height,
+                                   const nxs_camera *left, const nxs_camera *right, uint32_t width,
+                                   uint32_t height, uint8_t *d_left, uint8_t *d_right,
+                                   void *stream);
 
 /* NxStereo.Filter.despeckle/2 (lib/nx_stereo/filter.ex:14-80); radius 1..8. */
 nxs_status nxs_despeckle_device(const float *d_disparity, uint32_t width, uint32_t height,

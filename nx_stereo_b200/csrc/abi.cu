@@ -390,6 +390,28 @@ extern "C" nxs_status nxs_census_device(const uint8_t *d_image, uint32_t width, 
                : NXS_OK;
 }
 
+extern "C" nxs_status nxs_census_pair_device(const uint8_t *d_left, const uint8_t *d_right,
+                                             uint32_t width, uint32_t height,
+                                             uint64_t *d_left_codes, uint64_t *d_right_codes,
+                                             void *stream) {
+    CHECK_SIZE(d_left && d_right && d_left_codes && d_right_codes && width > 0 && height > 0);
+    return launch_census(d_left, d_right, width, height, d_left_codes, d_right_codes,
+                         static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_check_median_device(const float *d_disparity, const uint32_t *d_keys,
+                                              uint32_t width, uint32_t height,
+                                              uint32_t stage_mask, float *d_filtered,
+                                              void *stream) {
+    CHECK_SIZE(d_disparity && d_keys && d_filtered && width > 0 && width <= 4096 && height > 0);
+    return launch_check_median(d_disparity, d_keys, width, height, stage_mask ? 1 : 0,
+                               d_filtered, static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
 extern "C" nxs_status nxs_costs_device(const uint64_t *d_left_codes,
                                        const uint64_t *d_right_codes, uint32_t width,
                                        uint32_t height, uint32_t disparities, uint8_t *d_costs,
@@ -537,6 +559,21 @@ extern "C" nxs_status nxs_rectify_device(const uint8_t *d_frame, uint32_t frame_
                frame_width >= width && frame_height >= height);
     return launch_rectify(d_frame, frame_width, frame_height, to_camera(camera), width, height,
                           d_rectified, static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_rectify_pair_device(const uint8_t *d_left_frame,
+                                              const uint8_t *d_right_frame, uint32_t frame_width,
+                                              uint32_t frame_height, const nxs_camera *left,
+                                              const nxs_camera *right, uint32_t width,
+                                              uint32_t height, uint8_t *d_left, uint8_t *d_right,
+                                              void *stream) {
+    CHECK_SIZE(d_left_frame && d_right_frame && left && right && d_left && d_right &&
+               width > 0 && height > 0 && frame_width >= width && frame_height >= height);
+    return launch_rectify_pair(d_left_frame, d_right_frame, frame_width, frame_height,
+                               to_camera(left), to_camera(right), width, height, d_left, d_right,
+                               static_cast<cudaStream_t>(stream))
                ? NXS_CUDA_ERROR
                : NXS_OK;
 }
@@ -1136,9 +1173,9 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
         if (e) break;
         switch (m.kind) {
         case Kind::Rectification:
-            for (int side = 0; side < 2 && !e; ++side)
-                e = launch_rectify(slot.frames[side], g.frame_width, g.frame_height,
-                                   l.cameras[side], g.width, g.height, slot.images[side], s);
+            e = launch_rectify_pair(slot.frames[0], slot.frames[1], g.frame_width, g.frame_height,
+                                    l.cameras[0], l.cameras[1], g.width, g.height,
+                                    slot.images[0], slot.images[1], s);
             break;
         case Kind::Disparity: {
             MatcherScratch ms =

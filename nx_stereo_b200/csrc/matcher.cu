@@ -289,6 +289,75 @@ cudaError_t launch_median3(const float *image, int width, int height, int stage_
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------- check + median
+// The left-right check and the median in one pass over bands of kBandRows
+// rows: a block builds, in shared memory, the right maps and the checked
+// disparities of its band's rows and of the row above and below (rows
+// clamped at the image's edges, as the median replicates them), then filters
+// its rows. The per-pixel steps are consistency_row's and median_at's.
+constexpr int kBandRows = 1;
+
+size_t check_median_shared_bytes(int width) {
+    return (size_t)(kBandRows + 2) * width * (sizeof(uint32_t) + sizeof(float));
+}
+
+__global__ void __launch_bounds__(256)
+    check_median_kernel(const float *__restrict__ disparity, const uint32_t *__restrict__ keys,
+                        int width, int height, int stage_mask, float *__restrict__ filtered) {
+    extern __shared__ uint32_t band[];
+    constexpr int ROWS = kBandRows + 2;
+    uint32_t *right = band;                                     // [ROWS][width]
+    float *checked = reinterpret_cast<float *>(band + ROWS * width);  // [ROWS][width]
+    const int y0 = blockIdx.x * kBandRows;
+    const int cells = ROWS * width;
+    for (int i = threadIdx.x; i < cells; i += blockDim.x) right[i] = kInvalidKey;
+    __syncthreads();
+    for (int i = threadIdx.x; i < cells; i += blockDim.x) {
+        const int r = i / width, x = i % width;
+        const int y = min(max(y0 - 1 + r, 0), height - 1);
+        const uint32_t key = __ldcg(keys + (size_t)y * width + x);
+        if (key == kInvalidKey) continue;
+        const int winner = (int)(key & 0xFFFFu);
+        if (x - winner < 0) continue;  // a winner is at most x (past-edge costs lose)
+        atomicMin(&right[r * width + x - winner], (key & 0xFFFF0000u) | (65535u - (uint32_t)winner));
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < cells; i += blockDim.x) {
+        const int r = i / width, x = i % width;
+        const int y = min(max(y0 - 1 + r, 0), height - 1);
+        checked[i] = consistent_value<false>(__ldcg(disparity + (size_t)y * width + x), x, width,
+                                             right + r * width);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kBandRows * width; i += blockDim.x) {
+        const int ry = i / width, x = i % width, y = y0 + ry;
+        if (y >= height) break;
+        float v[9];
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int sx = min(max(x + dx, 0), width - 1);
+                v[(dy + 1) * 3 + dx + 1] = checked[(ry + 1 + dy) * width + sx];
+            }
+        filtered[(size_t)y * width + x] = median_of_nine(v, stage_mask);
+    }
+}
+
+cudaError_t launch_check_median(const float *disparity, const uint32_t *keys, int width,
+                                int height, int stage_mask, float *filtered,
+                                cudaStream_t stream) {
+    const size_t shared = check_median_shared_bytes(width);
+    // Wide images need more than the default 48 KB: allowed once, for the widest.
+    static const cudaError_t allowed = cudaFuncSetAttribute(
+        check_median_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int)check_median_shared_bytes(4096));
+    if (shared > 48 * 1024 && allowed) return allowed;
+    check_median_kernel<<<(height + kBandRows - 1) / kBandRows, 256, shared, stream>>>(
+        disparity, keys, width, height, stage_mask, filtered);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------- the matcher
 static size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
@@ -337,8 +406,7 @@ cudaError_t run_matcher(const uint8_t *left, const uint8_t *right, int width, in
     if ((e = launch_select_paths(s.paths, width, height, disparities, paths, uniqueness,
                                  s.selected, s.keys, stream, span)))
         return e;
-    if ((e = launch_consistency(s.selected, s.keys, width, height, s.checked, stream))) return e;
-    return launch_median3(s.checked, width, height, stage_mask, disparity, stream);
+    return launch_check_median(s.selected, s.keys, width, height, stage_mask, disparity, stream);
 }
 
 }  // namespace nxs

@@ -49,10 +49,18 @@ cudaError_t launch_select_sums(const uint16_t *sums, int width, int height, int 
                                cudaStream_t stream);
 cudaError_t launch_consistency(const float *disparity, const uint32_t *keys, int width,
                                int height, float *checked, cudaStream_t stream);
+// The left-right check and the median (with the stage mask) in one pass.
+cudaError_t launch_check_median(const float *disparity, const uint32_t *keys, int width,
+                                int height, int stage_mask, float *filtered, cudaStream_t stream);
 cudaError_t launch_median3(const float *image, int width, int height, int stage_mask,
                            float *filtered, cudaStream_t stream);
 
 // ---- the stages around it ----
+// Both sides of a pair in one launch (scale as launch_rectify).
+cudaError_t launch_rectify_pair(const uint8_t *left_frame, const uint8_t *right_frame,
+                                int frame_width, int frame_height, const Camera &left_camera,
+                                const Camera &right_camera, int width, int height,
+                                uint8_t *left, uint8_t *right, cudaStream_t stream);
 cudaError_t launch_rectify(const uint8_t *frame, int frame_width, int frame_height,
                            const Camera &camera, int width, int height, uint8_t *rectified,
                            cudaStream_t stream);

@@ -657,6 +657,21 @@ __device__ __forceinline__ void exchange(float &a, float &b) {
     b = hi;
 }
 
+// The middle of nine values by the network; then, for Stage.Disparity,
+// disparity <= 0 becomes -1.
+__device__ __forceinline__ float median_of_nine(float *v, int stage_mask) {
+    exchange(v[1], v[2]); exchange(v[4], v[5]); exchange(v[7], v[8]);
+    exchange(v[0], v[1]); exchange(v[3], v[4]); exchange(v[6], v[7]);
+    exchange(v[1], v[2]); exchange(v[4], v[5]); exchange(v[7], v[8]);
+    exchange(v[0], v[3]); exchange(v[5], v[8]); exchange(v[4], v[7]);
+    exchange(v[3], v[6]); exchange(v[1], v[4]); exchange(v[2], v[5]);
+    exchange(v[4], v[7]); exchange(v[4], v[2]); exchange(v[6], v[4]);
+    exchange(v[4], v[2]);
+    float out = v[4];
+    if (stage_mask && !(out > 0.0f)) out = -1.0f;
+    return out;
+}
+
 __device__ __forceinline__ void median_at(const float *__restrict__ image, int width,
                                           int height, int stage_mask,
                                           float *__restrict__ filtered, int x, int y) {
@@ -669,16 +684,7 @@ __device__ __forceinline__ void median_at(const float *__restrict__ image, int w
             int sy = min(max(y + dy, 0), height - 1), sx = min(max(x + dx, 0), width - 1);
             v[(dy + 1) * 3 + dx + 1] = __ldcg(image + (size_t)sy * width + sx);
         }
-    exchange(v[1], v[2]); exchange(v[4], v[5]); exchange(v[7], v[8]);
-    exchange(v[0], v[1]); exchange(v[3], v[4]); exchange(v[6], v[7]);
-    exchange(v[1], v[2]); exchange(v[4], v[5]); exchange(v[7], v[8]);
-    exchange(v[0], v[3]); exchange(v[5], v[8]); exchange(v[4], v[7]);
-    exchange(v[3], v[6]); exchange(v[1], v[4]); exchange(v[2], v[5]);
-    exchange(v[4], v[7]); exchange(v[4], v[2]); exchange(v[6], v[4]);
-    exchange(v[4], v[2]);
-    float out = v[4];
-    if (stage_mask && !(out > 0.0f)) out = -1.0f;
-    filtered[(size_t)y * width + x] = out;
+    filtered[(size_t)y * width + x] = median_of_nine(v, stage_mask);
 }
 
 }  // namespace nxs

@@ -15,11 +15,10 @@ namespace nxs {
 // native/stereo_match/src/rectify.rs:116-121) and the camera matrix; it is
 // scaled to the frame size at pixel centres and sampled bilinearly with 0
 // outside, then rounded half away from zero and clipped to u8.
-__global__ void rectify_kernel(const uint8_t *__restrict__ frame, int frame_width,
-                               int frame_height, const Camera camera, float scale_x,
-                               float scale_y, int width, uint8_t *__restrict__ rectified) {
-    const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    const int v = blockIdx.y;
+__device__ __forceinline__ void rectify_at(const uint8_t *__restrict__ frame, int frame_width,
+                                           int frame_height, const Camera &camera, float scale_x,
+                                           float scale_y, int width,
+                                           uint8_t *__restrict__ rectified, int u, int v) {
     if (u >= width) return;
     const float uf = (float)u, vf = (float)v;
     const float *ir = camera.inverse_pr;
@@ -60,6 +59,47 @@ __global__ void rectify_kernel(const uint8_t *__restrict__ frame, int frame_widt
     float r = roundf(value);
     r = r < 0.0f ? 0.0f : (r > 255.0f ? 255.0f : r);
     rectified[(size_t)v * width + u] = (uint8_t)r;
+}
+
+__global__ void rectify_kernel(const uint8_t *__restrict__ frame, int frame_width,
+                               int frame_height, const Camera camera, float scale_x,
+                               float scale_y, int width, uint8_t *__restrict__ rectified) {
+    rectify_at(frame, frame_width, frame_height, camera, scale_x, scale_y, width, rectified,
+               blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
+}
+
+// Both sides of a pair in one launch: blockIdx.z picks the side.
+struct RectifySides {
+    const uint8_t *frame[2];
+    uint8_t *rectified[2];
+    Camera camera[2];
+};
+
+__global__ void rectify_pair_kernel(const RectifySides sides, int frame_width, int frame_height,
+                                    float scale_x, float scale_y, int width) {
+    const int side = blockIdx.z;
+    rectify_at(sides.frame[side], frame_width, frame_height, sides.camera[side], scale_x,
+               scale_y, width, sides.rectified[side], blockIdx.x * blockDim.x + threadIdx.x,
+               blockIdx.y);
+}
+
+cudaError_t launch_rectify_pair(const uint8_t *left_frame, const uint8_t *right_frame,
+                                int frame_width, int frame_height, const Camera &left_camera,
+                                const Camera &right_camera, int width, int height,
+                                uint8_t *left, uint8_t *right, cudaStream_t stream) {
+    RectifySides sides;
+    sides.frame[0] = left_frame;
+    sides.frame[1] = right_frame;
+    sides.rectified[0] = left;
+    sides.rectified[1] = right;
+    sides.camera[0] = left_camera;
+    sides.camera[1] = right_camera;
+    const float scale_x = (float)((double)frame_width / (double)width);
+    const float scale_y = (float)((double)frame_height / (double)height);
+    dim3 grid((width + 127) / 128, height, 2);
+    rectify_pair_kernel<<<grid, 128, 0, stream>>>(sides, frame_width, frame_height, scale_x,
+                                                  scale_y, width);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_rectify(const uint8_t *frame, int frame_width, int frame_height,

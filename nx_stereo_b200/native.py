@@ -120,6 +120,8 @@ SIGNATURES = {
     "nxs_set_path_words": (_i, [_u32, _u32]),
     "nxs_path_words": (_u32, [_u32]),
     "nxs_census_device": (_i, [_P, _u32, _u32, _P, _P]),
+    "nxs_census_pair_device": (_i, [_P, _P, _u32, _u32, _P, _P, _P]),
+    "nxs_check_median_device": (_i, [_P, _P, _u32, _u32, _u32, _P, _P]),
     "nxs_costs_device": (_i, [_P, _P, _u32, _u32, _u32, _P, _P]),
     "nxs_aggregate_device": (_i, [_P, _P, _u32, _u32, _u32, _u32, _u32, _u32, _P, _P]),
     "nxs_paths_device": (_i, [_P, _u32, _u32, _u32, _u32, _u32, _u32, _P, _P]),
@@ -132,6 +134,8 @@ SIGNATURES = {
     "nxs_consistency_device": (_i, [_P, _P, _u32, _u32, _P, _P]),
     "nxs_median3_device": (_i, [_P, _u32, _u32, _u32, _P, _P]),
     "nxs_rectify_device": (_i, [_P, _u32, _u32, ctypes.POINTER(Camera), _u32, _u32, _P, _P]),
+    "nxs_rectify_pair_device": (_i, [_P, _P, _u32, _u32, ctypes.POINTER(Camera),
+                                     ctypes.POINTER(Camera), _u32, _u32, _P, _P, _P]),
     "nxs_despeckle_device": (_i, [_P, _u32, _u32, _f, _f, _u32, _P, _P]),
     "nxs_temporal_device": (_i, [_P, _P, _P, _u64, _f, _f, _f, _f, _P]),
     "nxs_depth_device": (_i, [_P, _u64, _f, _f, _P, _P, _P]),
