@@ -45,7 +45,7 @@ KERNELS_PER_STEP = 9  # rectify, census, costs, paths, select, check+median, des
 SERVING_CAP = None
 # DRAM bytes (read + write) of one path-aggregation launch on this workload, from
 # an ncu capture of this command (dram__bytes_read.sum + dram__bytes_write.sum).
-PATHS_TRAFFIC_BYTES = 113_165_568 + 349_915_392
+PATHS_TRAFFIC_BYTES = 108_585_728 + 349_709_824
 
 
 def parse():
@@ -327,8 +327,8 @@ def run_ours(args, rank, world, local_rank):
                      "algorithmic_bytes_per_launch": paths_bytes,
                      "avg_launch_ms": round(paths_avg_s * 1000, 4),
                      "traffic": PATHS_TRAFFIC_BYTES,
-                     "limiter": "integer ALU pipe (68.6% of peak issue under ncu); HBM at "
-                                "35% of peak"},
+                     "limiter": "the latency of each scan-line step with ~8 warps a SM (ncu: "
+                                "issue 59%, integer ALU pipe 54%, FMA pipe 16%, HBM 39%)"},
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "pipeline_roofline": {"b_alg_per_pair": b_alg,
                               "achieved_gbs": round(b_alg * value / world / 1e9, 1),
