@@ -22,6 +22,7 @@ percentile rule of the reference's stream benchmark, index ceil(n p) - 1
 (test/bench/stream.exs:223).
 """
 import collections
+import gc
 import heapq
 import math
 import time
@@ -268,7 +269,20 @@ def poisson_arrivals(count, rate_hz, duration_s, seed=0):
 def run_load(server, stream_ids, frames_of, arrivals, lead_s=0.02):
     """Submits each arrival (t, stream index) at its time and collects every
     result. Returns {latencies_ms, pairs, seconds, pairs_per_s, p50_ms, p99_ms,
-    max_in_flight}. frames_of[stream index] cycles through that stream's pairs."""
+    max_in_flight}. frames_of[stream index] cycles through that stream's pairs.
+    The interpreter's cyclic garbage collector is paused while the loop runs
+    (after one collection), so that none of its passes stalls the loop."""
+    gc_was_enabled = gc.isenabled()
+    gc.collect()
+    gc.disable()
+    try:
+        return _run_load(server, stream_ids, frames_of, arrivals, lead_s)
+    finally:
+        if gc_was_enabled:
+            gc.enable()
+
+
+def _run_load(server, stream_ids, frames_of, arrivals, lead_s):
     counters = collections.Counter()
     pending = list(arrivals)
     heapq.heapify(pending)
