@@ -250,15 +250,15 @@ nxs_status nxs_costs_device(const uint64_t *d_left_codes, const uint64_t *d_righ
 
 /* The sum of the path costs over every direction, u16
  * [height][width][disparities] (lib/nx_stereo.ex:544-606); disparities a
- * multiple of 32, at most 256. Uses the context's scratch. */
+ * multiple of 32 from 64 to 256. Uses the context's scratch. */
 nxs_status nxs_aggregate_device(nxs_context *context, const uint8_t *d_costs, uint32_t width,
                                 uint32_t height, uint32_t disparities, uint32_t paths,
                                 uint32_t p1, uint32_t p2, uint16_t *d_sums, void *stream);
 
 /* Each direction's path costs, u8 [paths][height][width][disparities], the
  * directions in the reference's order (lib/nx_stereo.ex:544-606): one warp per
- * scan line. d_paths holds `paths` volumes; disparities a multiple of 32,
- * at most 256. */
+ * scan line. d_paths holds `paths` volumes; disparities a multiple of 32
+ * from 64 to 256. */
 nxs_status nxs_paths_device(const uint8_t *d_costs, uint32_t width, uint32_t height,
                             uint32_t disparities, uint32_t paths, uint32_t p1, uint32_t p2,
                             uint8_t *d_paths, void *stream);

@@ -429,7 +429,7 @@ extern "C" nxs_status nxs_aggregate_device(nxs_context *c, const uint8_t *d_cost
                                            uint32_t paths, uint32_t p1, uint32_t p2,
                                            uint16_t *d_sums, void *stream) {
     CHECK_SIZE(c && d_costs && d_sums && width > 0 && height > 0 && disparities % 32 == 0 &&
-               disparities >= 32 && disparities <= 256 && (paths == 3 || paths == 8) &&
+               disparities >= 64 && disparities <= 256 && (paths == 3 || paths == 8) &&
                p1 < p2 && p2 + 48 <= 127);
     cudaSetDevice(c->device);
     std::lock_guard<std::mutex> g(c->lock);
@@ -447,7 +447,7 @@ extern "C" nxs_status nxs_paths_device(const uint8_t *d_costs, uint32_t width, u
                                        uint32_t disparities, uint32_t paths, uint32_t p1,
                                        uint32_t p2, uint8_t *d_paths, void *stream) {
     CHECK_SIZE(d_costs && d_paths && width > 0 && height > 0 && disparities % 32 == 0 &&
-               disparities >= 32 && disparities <= 256 && (paths == 3 || paths == 8) &&
+               disparities >= 64 && disparities <= 256 && (paths == 3 || paths == 8) &&
                p1 < p2 && p2 + 48 <= 127);
     return launch_paths(d_costs, width, height, disparities, paths, p1, p2, d_paths,
                         static_cast<cudaStream_t>(stream))
@@ -491,7 +491,7 @@ extern "C" nxs_status nxs_paths_device_ordered(const uint8_t *d_costs, uint32_t 
                                                uint32_t paths, uint32_t p1, uint32_t p2,
                                                uint32_t span, uint8_t *d_paths, void *stream) {
     CHECK_SIZE(d_costs && d_paths && width > 0 && height > 0 && disparities % 32 == 0 &&
-               disparities >= 32 && disparities <= 256 && (paths == 3 || paths == 8) &&
+               disparities >= 64 && disparities <= 256 && (paths == 3 || paths == 8) &&
                p1 < p2 && p2 + 48 <= 127 && (span == 0 || span == 8 || span == 16));
     return launch_paths(d_costs, width, height, disparities, paths, p1, p2, d_paths,
                         static_cast<cudaStream_t>(stream), (int)span)

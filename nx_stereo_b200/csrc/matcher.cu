@@ -167,6 +167,10 @@ cudaError_t launch_paths(const uint8_t *costs, int width, int height, int dispar
     else if (span == 16 && words == 4) words = 8;
     const bool permuted = span != 0;
     const int g = path_lanes(disparities, words);
+    // The kernels take 2..8 lanes a line at 16 words, 4..16 at 8 and 8..32 at
+    // 4 (64 to 256 disparities); fewer would be launched with the wrong shape.
+    if (g < (words == 16 ? 2 : words == 8 ? 4 : 8) || g > 256 / (2 * words))
+        return cudaErrorInvalidValue;
     PathSetup s;
     const int total = path_setup(width, height, disparities, paths, p1, p2, g, &s);
     if (words == 16) {

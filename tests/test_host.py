@@ -58,6 +58,20 @@ def test_sgm_check_refuses_what_nx_stereo_refuses():
     assert "p1 < p2" in native.check_sgm(64, 48, p1=64, p2=64).message
 
 
+def test_device_path_entries_refuse_disparities_their_kernels_do_not_cover():
+    # The path kernels hold 8 to 32 disparities a lane in 2 to 32 lanes a scan
+    # line: 64 to 256 disparities in steps of 32. The refusal comes before any
+    # device work, so fake non-null pointers never reach a kernel.
+    for d in (0, 32, 48, 80, 288):
+        calls = [("nxs_paths_device", (1, 8, 8, d, 8, 8, 64, 1, None)),
+                 ("nxs_paths_device_ordered", (1, 8, 8, d, 8, 8, 64, 16, 1, None)),
+                 ("nxs_aggregate_device", (1, 1, 8, 8, d, 8, 8, 64, 1, None))]
+        for name, args in calls:
+            with pytest.raises(native.NativeError) as refused:
+                native.call(name, *args)
+            assert refused.value.status == native.BAD_ARGUMENT, (name, d)
+
+
 # ---------------------------------------------------------------- stage settings
 GEOMETRY = {"width": 4, "height": 2, "frame_width": 6, "frame_height": 3,
             "focal_length_px": 100.0, "baseline_m": 0.1, "principal_point": (2.0, 1.0)}
