@@ -22,6 +22,7 @@ camera streams with Poisson arrivals at 30 pairs/s each: p50/p99 latency).
 threads, one pair per thread per step.
 """
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -39,6 +40,7 @@ METRIC = "pairs/s at 728x544x128 d, 8 paths (full frame-to-depth pipeline)"
 WIDTH, HEIGHT, DISPARITIES, PATHS = 728, 544, 128, 8
 DECIMATION = 4
 KERNELS_PER_STEP = 9  # rectify, census, costs, paths, select, check+median, despeckle, depth, cloud
+PATHS_EVERY = 4  # timed steps between those whose path kernel is bracketed by events
 # At most this many pairs on the device at once in the serving run, oldest
 # arrival first (None: up to every stream's request slots; caps of 4, 8 and 16
 # kept p99 at 30 pairs/s/stream the same and lowered the saturation rate).
@@ -179,13 +181,16 @@ class DevicePipeline:
               "despeckle", "depth", "cloud"]
 
     def step(self, frames, marks=None):
-        """One pair; `marks` (len(STAGES) + 1 CUDA events) bracket the stages."""
+        """One pair; `marks` (len(STAGES) + 1 CUDA events or None) bracket the
+        stages. An event between two kernels also ends the overlap of the
+        second's launch with the first's tail (programmatic dependent launch),
+        so the timed steps record only the step's ends and the path stage."""
         import ctypes
 
         s, call = self.stream, self.native.call
 
         def mark(i):
-            if marks is not None:
+            if marks is not None and marks[i] is not None:
                 marks[i].record()
 
         mark(0)
@@ -244,8 +249,16 @@ def run_ours(args, rank, world, local_rank):
         sampler.start()
         time.sleep(0.3)
         n_marks = len(DevicePipeline.STAGES) + 1
-        marks = [[torch.cuda.Event(enable_timing=True) for _ in range(n_marks)]
-                 for _ in range(args.steps)]
+        paths_at = DevicePipeline.STAGES.index("paths")
+        # Every step records its ends; every PATHS_EVERY-th also brackets the path
+        # kernel (each event between kernels costs ~2.5 us a step).
+        ends, with_paths = (0, n_marks - 1), (0, paths_at, paths_at + 1, n_marks - 1)
+
+        def events(which):
+            return [[torch.cuda.Event(enable_timing=True) if k in which(i) else None
+                     for k in range(n_marks)] for i in range(args.steps)]
+
+        marks = events(lambda i: with_paths if i % PATHS_EVERY == 0 else ends)
         torch.cuda.synchronize()
         t0 = time.monotonic()
         for i in range(args.steps):
@@ -254,9 +267,16 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         t1 = time.monotonic()
         step_ms = [m[0].elapsed_time(m[-1]) for m in marks]
-        stage_ms = {name: statistics.mean(m[k].elapsed_time(m[k + 1]) for m in marks)
+        paths_ms = [m[paths_at].elapsed_time(m[paths_at + 1]) for m in marks
+                    if m[paths_at] is not None]
+        # Each stage's time from a second, untimed run with an event at every stage.
+        stage_marks = events(lambda i: range(n_marks))
+        for i in range(args.steps):
+            flush.fill_(i & 0xFF)
+            pipe.step(d_frames[i % len(d_frames)], stage_marks[i])
+        torch.cuda.synchronize()
+        stage_ms = {name: statistics.mean(m[k].elapsed_time(m[k + 1]) for m in stage_marks)
                     for k, name in enumerate(DevicePipeline.STAGES)}
-        paths_ms = [m[3].elapsed_time(m[4]) for m in marks]
     total_s = replicas.max_over_ranks(sum(step_ms) / 1000.0, device="cuda")
     value = replicas.whole_job_rate(args.steps, world, total_s)
 
@@ -293,10 +313,19 @@ def run_ours(args, rank, world, local_rank):
     e2e_loop(max(args.warmup, mod.depth()))
     torch.cuda.synchronize()
     replicas.barrier()
-    e0 = time.perf_counter()
-    e2e_loop(args.steps)
-    torch.cuda.synchronize()
-    e_s = replicas.max_over_ranks(time.perf_counter() - e0, device="cuda")
+    # The cyclic collector paused for the timed loop, as the serving loop does:
+    # a collection of the replies' objects stalls the host for milliseconds.
+    collecting = gc.isenabled()
+    gc.disable()
+    try:
+        e0 = time.perf_counter()
+        e2e_loop(args.steps)
+        torch.cuda.synchronize()
+        e_elapsed = time.perf_counter() - e0
+    finally:
+        if collecting:
+            gc.enable()
+    e_s = replicas.max_over_ranks(e_elapsed, device="cuda")
     sampler.stop()
     clocks = sampler.summary(t0, t1)
     seg.release()
@@ -330,6 +359,7 @@ def run_ours(args, rank, world, local_rank):
                      "limiter": "the latency of each scan-line step with ~8 warps a SM (ncu: "
                                 "issue 59%, integer ALU pipe 54%, FMA pipe 16%, HBM 39%)"},
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+        "stages_ms_from": "a second run of the same steps with an event between every stage",
         "pipeline_roofline": {"b_alg_per_pair": b_alg,
                               "achieved_gbs": round(b_alg * value / world / 1e9, 1),
                               "frac": round(b_alg * value / world / 1e9 / peak, 4)},
@@ -337,7 +367,7 @@ def run_ours(args, rank, world, local_rank):
                 "unit": "pairs/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "CudaSegment.send_request/await_ (C ABI nxs_run_async), depth "
-                       f"{mod.depth()}"},
+                       f"{mod.depth()}, cyclic garbage collector paused while timed"},
         "clocks": clocks,
     }
     return line

@@ -24,6 +24,7 @@ __global__ void __launch_bounds__(kCensusX *kCensusY)
     census_kernel(const uint8_t *__restrict__ left, const uint8_t *__restrict__ right, int width,
                   int height, uint64_t *__restrict__ left_codes,
                   uint64_t *__restrict__ right_codes) {
+    follow_previous_grid();
     __shared__ uint8_t tile[census_tile_bytes(kCensusY)];
     census_tile<kCensusY, kCensusX * kCensusY>(
         blockIdx.z == 0 ? left : right, width, height,
@@ -36,9 +37,8 @@ cudaError_t launch_census(const uint8_t *left, const uint8_t *right, int width, 
     dim3 block(kCensusX, kCensusY);
     dim3 grid((width + kCensusX - 1) / kCensusX, (height + kCensusY - 1) / kCensusY,
               right ? 2 : 1);
-    census_kernel<<<grid, block, 0, stream>>>(left, right, width, height, left_codes,
-                                              right_codes);
-    return cudaGetLastError();
+    return launch_after(census_kernel, grid, block, 0, stream, left, right, width, height,
+                        left_codes, right_codes);
 }
 
 // ---------------------------------------------------------------- costs
@@ -46,6 +46,7 @@ template <int SPAN>
 __global__ void __launch_bounds__(128)
     costs_kernel(const uint64_t *__restrict__ left_codes, const uint64_t *__restrict__ right_codes,
                  int width, int disparities, uint8_t *__restrict__ costs) {
+    follow_previous_grid();
     extern __shared__ __align__(16) uint8_t staged[];
     costs_tile<SPAN>(left_codes, right_codes, width, disparities, costs,
                      blockIdx.x * kCostPixels, blockIdx.y, staged);
@@ -57,8 +58,8 @@ cudaError_t launch_costs(const uint64_t *left_codes, const uint64_t *right_codes
     dim3 grid((width + kCostPixels - 1) / kCostPixels, height);
     const size_t shared = costs_shared_bytes(disparities);
 #define NXS_COSTS(S)                                                                          \
-    costs_kernel<S><<<grid, 128, shared, stream>>>(left_codes, right_codes, width, disparities, \
-                                                   costs)
+    launch_after(costs_kernel<S>, grid, dim3(128), shared, stream, left_codes, right_codes,   \
+                 width, disparities, costs)
     if (span == 16) NXS_COSTS(16);
     else if (span == 8) NXS_COSTS(8);
     else NXS_COSTS(0);
@@ -72,6 +73,7 @@ template <int G, int WORDS, bool FULL, int SPAN>
 __global__ void __launch_bounds__(32)
     paths_kernel(const uint8_t *__restrict__ costs, uint8_t *__restrict__ paths_out,
                  const PathSetup s) {
+    follow_previous_grid();
     using Piece = typename std::conditional<WORDS == 4, uint2, uint4>::type;
     constexpr int PIECES = WORDS == 16 ? 2 : 1;
     __shared__ Piece ring[kPrefetch * PIECES][32];
@@ -134,13 +136,19 @@ int path_setup(int width, int height, int disparities, int paths, int p1, int p2
     return total;
 }
 
+// The path kernel is one wave of one-warp blocks whose time is set by the most
+// loaded SM. launch_after starts it as the costs kernel's last block exits, so
+// its blocks spread over idle SMs; with an early signal from every costs block
+// (griddepcontrol.launch_dependents at their start) they landed unevenly beside
+// the costs kernel's last wave and a pair took 525 us instead of 290.
 template <int WORDS, bool PERMUTED>
 static void launch_paths_in(const uint8_t *costs, uint8_t *paths_out, const PathSetup &s,
                             int total, int g, cudaStream_t stream) {
     constexpr int SPAN = PERMUTED ? (WORDS == 4 ? 8 : 16) : 0;
     const bool full = g * 2 * WORDS == s.disparities;
 #define NXS_PATHS(G, F)                                                                        \
-    paths_kernel<G, WORDS, F, SPAN><<<total, 32, 0, stream>>>(costs, paths_out, s)
+    launch_after(paths_kernel<G, WORDS, F, SPAN>, dim3(total), dim3(32), 0, stream, costs,    \
+                 paths_out, s)
     if constexpr (WORDS == 16) {
         if (g == 2) full ? NXS_PATHS(2, true) : NXS_PATHS(2, false);
         else if (g == 4) full ? NXS_PATHS(4, true) : NXS_PATHS(4, false);
@@ -189,6 +197,7 @@ cudaError_t launch_paths(const uint8_t *costs, int width, int height, int dispar
 // sums[y][x][d] = sum of the P path volumes, u16 (at most 8 x 127 = 1016).
 __global__ void sum_paths_kernel(const uint8_t *__restrict__ paths_in, size_t volume, int paths,
                                  uint16_t *__restrict__ sums) {
+    follow_previous_grid();
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     size_t quads = volume / 4;
     if (i >= quads) return;
@@ -205,9 +214,8 @@ cudaError_t launch_sum_paths(const uint8_t *paths_in, int width, int height, int
                              int paths, uint16_t *sums, cudaStream_t stream) {
     size_t volume = (size_t)width * height * disparities;
     size_t quads = volume / 4;
-    sum_paths_kernel<<<(unsigned)((quads + 255) / 256), 256, 0, stream>>>(paths_in, volume, paths,
-                                                                          sums);
-    return cudaGetLastError();
+    return launch_after(sum_paths_kernel, dim3((unsigned)((quads + 255) / 256)), dim3(256), 0,
+                        stream, paths_in, volume, paths, sums);
 }
 
 // ---------------------------------------------------------------- select
@@ -217,6 +225,7 @@ __global__ void __launch_bounds__(128)
     select_kernel(const void *__restrict__ source, int width, int height, int disparities,
                   size_t volume, float uniqueness, float *__restrict__ disparity,
                   uint32_t *__restrict__ keys, uint32_t one) {
+    follow_previous_grid();
     __shared__ __align__(16) uint16_t values_of[128 / G][256];
     select_pixels<G, PATHS, SPAN>(source, width, height, disparities, volume, uniqueness,
                                   disparity, keys, nullptr, blockIdx.x, values_of, one);
@@ -231,8 +240,8 @@ static cudaError_t launch_select(const void *source, int width, int height, int 
     const int g = group_lanes(disparities);
     const unsigned blocks = (unsigned)((pixels + 128 / g - 1) / (128 / g));
 #define NXS_SELECT(G)                                                                         \
-    select_kernel<G, PATHS, SPAN><<<blocks, 128, 0, stream>>>(                                \
-        source, width, height, disparities, volume, uniqueness, disparity, keys, 1u)
+    launch_after(select_kernel<G, PATHS, SPAN>, dim3(blocks), dim3(128), 0, stream, source,   \
+                 width, height, disparities, volume, uniqueness, disparity, keys, 1u)
     if (g == 4) NXS_SELECT(4);
     else if (g == 8) NXS_SELECT(8);
     else NXS_SELECT(16);
@@ -268,20 +277,21 @@ cudaError_t launch_select_sums(const uint16_t *sums, int width, int height, int 
 __global__ void __launch_bounds__(256)
     consistency_kernel(const float *__restrict__ disparity, const uint32_t *__restrict__ keys,
                        int width, float *__restrict__ checked) {
+    follow_previous_grid();
     extern __shared__ uint32_t right[];
     consistency_row(disparity, keys, width, checked, blockIdx.x, right);
 }
 
 cudaError_t launch_consistency(const float *disparity, const uint32_t *keys, int width,
                                int height, float *checked, cudaStream_t stream) {
-    consistency_kernel<<<height, 256, sizeof(uint32_t) * width, stream>>>(disparity, keys, width,
-                                                                         checked);
-    return cudaGetLastError();
+    return launch_after(consistency_kernel, dim3(height), dim3(256), sizeof(uint32_t) * width,
+                        stream, disparity, keys, width, checked);
 }
 
 // ---------------------------------------------------------------- median
 __global__ void median3_kernel(const float *__restrict__ image, int width, int height,
                                int stage_mask, float *__restrict__ filtered) {
+    follow_previous_grid();
     median_at(image, width, height, stage_mask, filtered, blockIdx.x * blockDim.x + threadIdx.x,
               blockIdx.y);
 }
@@ -289,8 +299,8 @@ __global__ void median3_kernel(const float *__restrict__ image, int width, int h
 cudaError_t launch_median3(const float *image, int width, int height, int stage_mask,
                            float *filtered, cudaStream_t stream) {
     dim3 grid((width + 127) / 128, height);
-    median3_kernel<<<grid, 128, 0, stream>>>(image, width, height, stage_mask, filtered);
-    return cudaGetLastError();
+    return launch_after(median3_kernel, grid, dim3(128), 0, stream, image, width, height,
+                        stage_mask, filtered);
 }
 
 // ---------------------------------------------------------------- check + median
@@ -308,6 +318,7 @@ size_t check_median_shared_bytes(int width) {
 __global__ void __launch_bounds__(256)
     check_median_kernel(const float *__restrict__ disparity, const uint32_t *__restrict__ keys,
                         int width, int height, int stage_mask, float *__restrict__ filtered) {
+    follow_previous_grid();
     extern __shared__ uint32_t band[];
     constexpr int ROWS = kBandRows + 2;
     uint32_t *right = band;                                     // [ROWS][width]
@@ -357,9 +368,9 @@ cudaError_t launch_check_median(const float *disparity, const uint32_t *keys, in
         check_median_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
         (int)check_median_shared_bytes(4096));
     if (shared > 48 * 1024 && allowed) return allowed;
-    check_median_kernel<<<(height + kBandRows - 1) / kBandRows, 256, shared, stream>>>(
-        disparity, keys, width, height, stage_mask, filtered);
-    return cudaGetLastError();
+    return launch_after(check_median_kernel, dim3((height + kBandRows - 1) / kBandRows),
+                        dim3(256), shared, stream, disparity, keys, width, height, stage_mask,
+                        filtered);
 }
 
 // ---------------------------------------------------------------- the matcher

@@ -4,6 +4,8 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
+
 #include <cuda_runtime.h>
 
 namespace nxs {
@@ -28,5 +30,37 @@ __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b)
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+
+// Programmatic dependent launch: a kernel launched by launch_after is launched
+// as the last block of the kernel before it on the stream exits, before that
+// grid's completion is processed, so the launch gap between stages overlaps
+// the previous stage's end. Such a kernel calls follow_previous_grid() before
+// it touches global memory: it waits until the grid before it has completed
+// and its writes are visible (griddepcontrol.wait, which returns at once when
+// nothing precedes the kernel programmatically). Since every kernel waits at
+// its top, a successor never runs ahead of any earlier kernel's writes, nor
+// overwrites what an earlier kernel still reads. No kernel signals its
+// successor earlier (griddepcontrol.launch_dependents): blocks launched early
+// sat resident while they waited, which with many streams in flight held SMs
+// other streams' kernels could use (serving saturation 2,455 -> 2,090 pairs/s).
+__device__ __forceinline__ void follow_previous_grid() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+template <typename... Params, typename... Args>
+inline cudaError_t launch_after(void (*kernel)(Params...), dim3 grid, dim3 block, size_t shared,
+                                cudaStream_t stream, Args &&...args) {
+    cudaLaunchConfig_t config = {};
+    config.gridDim = grid;
+    config.blockDim = block;
+    config.dynamicSmemBytes = shared;
+    config.stream = stream;
+    cudaLaunchAttribute attribute[1];
+    attribute[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attribute[0].val.programmaticStreamSerializationAllowed = 1;
+    config.attrs = attribute;
+    config.numAttrs = 1;
+    return cudaLaunchKernelEx(&config, kernel, std::forward<Args>(args)...);
+}
 
 }  // namespace nxs

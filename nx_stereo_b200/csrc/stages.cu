@@ -64,6 +64,7 @@ __device__ __forceinline__ void rectify_at(const uint8_t *__restrict__ frame, in
 __global__ void rectify_kernel(const uint8_t *__restrict__ frame, int frame_width,
                                int frame_height, const Camera camera, float scale_x,
                                float scale_y, int width, uint8_t *__restrict__ rectified) {
+    follow_previous_grid();
     rectify_at(frame, frame_width, frame_height, camera, scale_x, scale_y, width, rectified,
                blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
 }
@@ -77,6 +78,7 @@ struct RectifySides {
 
 __global__ void rectify_pair_kernel(const RectifySides sides, int frame_width, int frame_height,
                                     float scale_x, float scale_y, int width) {
+    follow_previous_grid();
     const int side = blockIdx.z;
     rectify_at(sides.frame[side], frame_width, frame_height, sides.camera[side], scale_x,
                scale_y, width, sides.rectified[side], blockIdx.x * blockDim.x + threadIdx.x,
@@ -97,9 +99,8 @@ cudaError_t launch_rectify_pair(const uint8_t *left_frame, const uint8_t *right_
     const float scale_x = (float)((double)frame_width / (double)width);
     const float scale_y = (float)((double)frame_height / (double)height);
     dim3 grid((width + 127) / 128, height, 2);
-    rectify_pair_kernel<<<grid, 128, 0, stream>>>(sides, frame_width, frame_height, scale_x,
-                                                  scale_y, width);
-    return cudaGetLastError();
+    return launch_after(rectify_pair_kernel, grid, dim3(128), 0, stream, sides, frame_width,
+                        frame_height, scale_x, scale_y, width);
 }
 
 cudaError_t launch_rectify(const uint8_t *frame, int frame_width, int frame_height,
@@ -109,9 +110,8 @@ cudaError_t launch_rectify(const uint8_t *frame, int frame_width, int frame_heig
     const float scale_x = (float)((double)frame_width / (double)width);
     const float scale_y = (float)((double)frame_height / (double)height);
     dim3 grid((width + 127) / 128, height);
-    rectify_kernel<<<grid, 128, 0, stream>>>(frame, frame_width, frame_height, camera, scale_x,
-                                             scale_y, width, rectified);
-    return cudaGetLastError();
+    return launch_after(rectify_kernel, grid, dim3(128), 0, stream, frame, frame_width,
+                        frame_height, camera, scale_x, scale_y, width, rectified);
 }
 
 // ---------------------------------------------------------------- despeckle
@@ -125,6 +125,7 @@ __global__ void __launch_bounds__(kSpeckleX *kSpeckleY)
     despeckle_kernel(const float *__restrict__ disparity, int width, int height,
                      float min_support, float max_diff, int radius,
                      float *__restrict__ despeckled) {
+    follow_previous_grid();
     extern __shared__ float window[];
     const int tw = kSpeckleX + 2 * radius, th = kSpeckleY + 2 * radius;
     const int x0 = blockIdx.x * kSpeckleX, y0 = blockIdx.y * kSpeckleY;
@@ -155,9 +156,8 @@ cudaError_t launch_despeckle(const float *disparity, int width, int height, floa
     dim3 block(kSpeckleX, kSpeckleY);
     dim3 grid((width + kSpeckleX - 1) / kSpeckleX, (height + kSpeckleY - 1) / kSpeckleY);
     size_t shared = sizeof(float) * (kSpeckleX + 2 * radius) * (kSpeckleY + 2 * radius);
-    despeckle_kernel<<<grid, block, shared, stream>>>(disparity, width, height, min_support,
-                                                      max_diff, radius, despeckled);
-    return cudaGetLastError();
+    return launch_after(despeckle_kernel, grid, block, shared, stream, disparity, width, height,
+                        min_support, max_diff, radius, despeckled);
 }
 
 // ---------------------------------------------------------------- temporal
@@ -165,6 +165,7 @@ cudaError_t launch_despeckle(const float *disparity, int width, int height, floa
 __global__ void temporal_kernel(float *__restrict__ disparity, float *__restrict__ previous,
                                 float *__restrict__ missed, size_t pixels, float alpha,
                                 float delta, float hold, float max_missed) {
+    follow_previous_grid();
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pixels) return;
     const float current = disparity[i], before = previous[i];
@@ -183,9 +184,9 @@ __global__ void temporal_kernel(float *__restrict__ disparity, float *__restrict
 cudaError_t launch_temporal(float *disparity, float *previous, float *missed, size_t pixels,
                             float alpha, float delta, float hold, float max_missed,
                             cudaStream_t stream) {
-    temporal_kernel<<<(unsigned)((pixels + 255) / 256), 256, 0, stream>>>(
-        disparity, previous, missed, pixels, alpha, delta, hold, max_missed);
-    return cudaGetLastError();
+    return launch_after(temporal_kernel, dim3((unsigned)((pixels + 255) / 256)), dim3(256), 0,
+                        stream, disparity, previous, missed, pixels, alpha, delta, hold,
+                        max_missed);
 }
 
 // ---------------------------------------------------------------- depth
@@ -194,6 +195,7 @@ cudaError_t launch_temporal(float *disparity, float *previous, float *missed, si
 __global__ void depth_kernel(const float *__restrict__ disparity, size_t pixels,
                              float focal_length_px, float baseline_m,
                              uint16_t *__restrict__ depth_mm, float *__restrict__ depth_m) {
+    follow_previous_grid();
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pixels) return;
     const float focal_baseline = fmul(focal_length_px, baseline_m);
@@ -207,9 +209,9 @@ __global__ void depth_kernel(const float *__restrict__ disparity, size_t pixels,
 cudaError_t launch_depth(const float *disparity, size_t pixels, float focal_length_px,
                          float baseline_m, uint16_t *depth_mm, float *depth_m,
                          cudaStream_t stream) {
-    depth_kernel<<<(unsigned)((pixels + 255) / 256), 256, 0, stream>>>(
-        disparity, pixels, focal_length_px, baseline_m, depth_mm, depth_m);
-    return cudaGetLastError();
+    return launch_after(depth_kernel, dim3((unsigned)((pixels + 255) / 256)), dim3(256), 0,
+                        stream, disparity, pixels, focal_length_px, baseline_m, depth_mm,
+                        depth_m);
 }
 
 // ---------------------------------------------------------------- cloud
@@ -219,6 +221,7 @@ __global__ void cloud_kernel(const float *__restrict__ depth_m, int width, int g
                              int grid_height, int decimation, float focal_length_px, float cx,
                              float cy, float nearest_m, float farthest_m,
                              float *__restrict__ grid, int32_t *__restrict__ kept) {
+    follow_previous_grid();
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     const int row = blockIdx.y;
     if (col >= grid_width || row >= grid_height) return;
@@ -247,10 +250,8 @@ cudaError_t launch_cloud(const float *depth_m, int width, int height, int decima
     if (e) return e;
     if (gw == 0 || gh == 0) return cudaSuccess;
     dim3 grid_dim((gw + 127) / 128, gh);
-    cloud_kernel<<<grid_dim, 128, 0, stream>>>(depth_m, width, gw, gh, decimation,
-                                               focal_length_px, cx, cy, nearest_m, farthest_m,
-                                               grid, kept);
-    return cudaGetLastError();
+    return launch_after(cloud_kernel, grid_dim, dim3(128), 0, stream, depth_m, width, gw, gh,
+                        decimation, focal_length_px, cx, cy, nearest_m, farthest_m, grid, kept);
 }
 
 // ---------------------------------------------------------------- quality
@@ -262,6 +263,7 @@ cudaError_t launch_cloud(const float *depth_m, int width, int height, int decima
 __global__ void quality_columns_kernel(const float *__restrict__ disparity,
                                        const float *__restrict__ previous, int width, int height,
                                        float *__restrict__ column_sums) {
+    follow_previous_grid();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= width) return;
     double acc[5] = {0, 0, 0, 0, 0};
@@ -283,6 +285,7 @@ __global__ void quality_columns_kernel(const float *__restrict__ disparity,
 
 __global__ void quality_total_kernel(const float *__restrict__ column_sums, int width,
                                      float *__restrict__ sums) {
+    follow_previous_grid();
     const int p = threadIdx.x;
     if (p >= 5) return;
     double total = 0.0;
@@ -292,10 +295,10 @@ __global__ void quality_total_kernel(const float *__restrict__ column_sums, int 
 
 cudaError_t launch_quality(const float *disparity, float *previous, int width, int height,
                            float *column_sums, float *sums, cudaStream_t stream) {
-    quality_columns_kernel<<<(width + 127) / 128, 128, 0, stream>>>(disparity, previous, width,
-                                                                    height, column_sums);
-    quality_total_kernel<<<1, 32, 0, stream>>>(column_sums, width, sums);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_after(quality_columns_kernel, dim3((width + 127) / 128), dim3(128), 0,
+                                 stream, disparity, previous, width, height, column_sums);
+    if (!e) e = launch_after(quality_total_kernel, dim3(1), dim3(32), 0, stream, column_sums,
+                             width, sums);
     if (e) return e;
     return cudaMemcpyAsync(previous, disparity, sizeof(float) * (size_t)width * height,
                            cudaMemcpyDeviceToDevice, stream);
