@@ -46,7 +46,7 @@ namespace {
 enum Phase { kCensus = 0, kCosts, kPaths, kSelect, kCheck, kMedian, kPhases };
 
 constexpr int kThreads = 128;
-constexpr int kCensusRows = 16;        // census tile: 32 x 16 pixels
+constexpr int kCensusRows = 4;         // census tile: 128 x 4 pixels (census4_tile)
 constexpr int kPixelsPerItem = 1024;   // check and median items
 // Control words: queue head, status, 2 unused, then 16 u64 cycle sums (each
 // phase's
@@ -193,14 +193,14 @@ __device__ __forceinline__ void work(const BatchPair *__restrict__ pairs,
         switch (phase) {
         case kCensus: {
             const int image = item / P.census_tiles, tile = item % P.census_tiles;
-            const int x0 = (tile % P.census_columns) * kCensusX;
+            const int x0 = (tile % P.census_columns) * kCensus4X;
             const int y0 = (tile / P.census_columns) * kCensusRows;
-            census_tile<kCensusRows, kThreads>(image ? P.right : P.left, W, H,
-                                               image ? P.right_codes : P.left_codes, x0, y0,
-                                               tid, smem);
+            census4_tile<kCensusRows, kThreads>(image ? P.right : P.left, W, H,
+                                                image ? P.right_codes : P.left_codes, x0, y0,
+                                                tid, smem);
             if (image == 0) {  // the right map of these pixels starts empty
-                for (int i = tid; i < kCensusX * kCensusRows; i += kThreads) {
-                    const int x = x0 + i % kCensusX, y = y0 + i / kCensusX;
+                for (int i = tid; i < kCensus4X * kCensusRows; i += kThreads) {
+                    const int x = x0 + i % kCensus4X, y = y0 + i / kCensus4X;
                     if (x < W && y < H) P.right_map[(size_t)y * W + x] = kInvalidKey;
                 }
             }
@@ -377,7 +377,7 @@ void shape_pair(const nxs_batch_pair &s, const nxs_batch_tuning &t, BatchPair *o
     P.select_lanes = group_lanes(D);
     P.path_words = t.path_words ? t.path_words : path_words(D);
     P.path_lanes = path_lanes(D, P.path_words);
-    P.census_columns = (W + kCensusX - 1) / kCensusX;
+    P.census_columns = (W + kCensus4X - 1) / kCensus4X;
     P.census_tiles = P.census_columns * ((H + kCensusRows - 1) / kCensusRows);
     P.cost_columns = (W + kCostPixels - 1) / kCostPixels;
     P.cost_rows = t.cost_rows;
@@ -665,7 +665,7 @@ nxs_status prepare(nxs_batch *b, const nxs_batch_tuning &t, char *error, size_t 
     b->shared_bytes = std::max({costs_shared_bytes(max_disparities),
                                 (size_t)(kThreads / 32) * kPrefetch * 32 * 2 * max_words,
                                 (size_t)(128 / 4) * 256 * sizeof(uint16_t),
-                                (size_t)census_tile_bytes(kCensusRows)});
+                                (size_t)census4_tile_bytes(kCensusRows)});
     int sms = 0, resident = 0;
     cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
     auto kernel = b->wide ? batch_kernel<true> : batch_kernel<false>;

@@ -20,25 +20,28 @@
 namespace nxs {
 
 // ---------------------------------------------------------------- census
-__global__ void __launch_bounds__(kCensusX *kCensusY)
+// A block of 256 threads takes 128 x 8 pixels of one image (blockIdx.z), four
+// pixels a thread.
+constexpr int kCensus4Rows = 8, kCensus4Threads = 256;
+
+__global__ void __launch_bounds__(kCensus4Threads)
     census_kernel(const uint8_t *__restrict__ left, const uint8_t *__restrict__ right, int width,
                   int height, uint64_t *__restrict__ left_codes,
                   uint64_t *__restrict__ right_codes) {
+    __shared__ __align__(16) uint8_t tile[census4_tile_bytes(kCensus4Rows)];
     follow_previous_grid();
-    __shared__ uint8_t tile[census_tile_bytes(kCensusY)];
-    census_tile<kCensusY, kCensusX * kCensusY>(
+    census4_tile<kCensus4Rows, kCensus4Threads>(
         blockIdx.z == 0 ? left : right, width, height,
-        blockIdx.z == 0 ? left_codes : right_codes, blockIdx.x * kCensusX, blockIdx.y * kCensusY,
-        threadIdx.y * kCensusX + threadIdx.x, tile);
+        blockIdx.z == 0 ? left_codes : right_codes, blockIdx.x * kCensus4X,
+        blockIdx.y * kCensus4Rows, threadIdx.x, tile);
 }
 
 cudaError_t launch_census(const uint8_t *left, const uint8_t *right, int width, int height,
                           uint64_t *left_codes, uint64_t *right_codes, cudaStream_t stream) {
-    dim3 block(kCensusX, kCensusY);
-    dim3 grid((width + kCensusX - 1) / kCensusX, (height + kCensusY - 1) / kCensusY,
+    dim3 grid((width + kCensus4X - 1) / kCensus4X, (height + kCensus4Rows - 1) / kCensus4Rows,
               right ? 2 : 1);
-    return launch_after(census_kernel, grid, block, 0, stream, left, right, width, height,
-                        left_codes, right_codes);
+    return launch_after(census_kernel, grid, dim3(kCensus4Threads), 0, stream, left, right,
+                        width, height, left_codes, right_codes);
 }
 
 // ---------------------------------------------------------------- costs

@@ -15,46 +15,106 @@ namespace nxs {
 // 9x7 sparse census (lib/nx_stereo.ex:491-505): bit i for the i-th neighbour
 // in row-major order over dy in -3..3, dx in -4..4, both non-zero, set where
 // neighbour + 1 < centre; borders replicated (lib/nx_stereo/image.ex:508-537).
-// A tile of 32 x ROWS pixels stages its window of 40 x (ROWS + 6) pixels in
-// shared memory (`tile`, at least census_tile_bytes(ROWS)); THREADS threads
-// share the work.
-constexpr int kCensusX = 32, kCensusY = 8;
 
-__host__ __device__ constexpr int census_tile_bytes(int rows) { return (rows + 6) * (kCensusX + 8); }
+// Four pixels' codes at once, as packed bytes. `window` holds the pixels'
+// 9x7 neighbourhoods in rows `pitch` bytes apart (pitch a multiple of 4);
+// the first pixel's centre is at row `centre_row`, column `col` (a multiple
+// of 4). The six neighbour rows give the code's six bytes: for each row, the
+// eight neighbours at dx -4..-1, 1..4 enter each pixel's byte from the top
+// (acc >> 1, the new bit at bit 7), so after eight the first is bit 0, as in
+// census_code. n + 1 < c is n < t with t = c - 1 (0 where c is 0: then no
+// neighbour is below it), compared four bytes at a time: bit 7 of
+// d = (n | 0x80) - (t & 0x7F) says low7(n) >= low7(t), and
+// n < t = (!n7 & t7) | (n7 == t7 & !d7).
+__device__ __forceinline__ void census4(const uint8_t *window, int pitch, int col,
+                                        int centre_row, uint64_t *codes) {
+    const uint32_t c =
+        *reinterpret_cast<const uint32_t *>(window + (size_t)centre_row * pitch + col);
+    const uint32_t zero = ~(((c & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | c | 0x7F7F7F7Fu);  // bit 7: c == 0
+    const uint32_t t = (c | (zero >> 7)) - 0x01010101u;
+    const uint32_t t_low = t & 0x7F7F7F7Fu;
+    uint32_t acc[6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+        const int dy = r < 3 ? r - 3 : r - 2;
+        const uint32_t *w =
+            reinterpret_cast<const uint32_t *>(window + (size_t)(centre_row + dy) * pitch + col - 4);
+        const uint32_t w0 = w[0], w1 = w[1], w2 = w[2];  // columns col - 4 .. col + 7
+        uint32_t a = 0;
+#pragma unroll
+        for (int dx = -4; dx <= 4; ++dx) {
+            if (dx == 0) continue;
+            // the four pixels' neighbours at dx: bytes col + dx .. col + dx + 3
+            const int o = dx + 4;  // offset from column col - 4
+            const uint32_t n = o == 0 ? w0 : o == 4 ? w1 : o == 8 ? w2
+                               : o < 4 ? __byte_perm(w0, w1, (o) | (o + 1) << 4 | (o + 2) << 8 | (o + 3) << 12)
+                                       : __byte_perm(w1, w2, (o - 4) | (o - 3) << 4 | (o - 2) << 8 | (o - 1) << 12);
+            const uint32_t d = (n | 0x80808080u) - t_low;
+            const uint32_t below = (~n & t) | (~(n ^ t) & ~d);  // bit 7 of each byte
+            a = ((a >> 1) & 0x7F7F7F7Fu) | (below & 0x80808080u);
+        }
+        acc[r] = a;
+    }
+    // pixel i: byte r of its code is byte i of acc[r]
+    const uint32_t lo01 = __byte_perm(acc[0], acc[1], 0x5140), lo23 = __byte_perm(acc[2], acc[3], 0x5140);
+    const uint32_t hi01 = __byte_perm(acc[0], acc[1], 0x7362), hi23 = __byte_perm(acc[2], acc[3], 0x7362);
+    const uint32_t top01 = __byte_perm(acc[4], acc[5], 0x5140), top23 = __byte_perm(acc[4], acc[5], 0x7362);
+    // lo01 = (a0.b0, a1.b0, a0.b1, a1.b1): pixel 0's bytes 0-1 in its low half, pixel 1's in its high
+    codes[0] = (uint64_t)__byte_perm(lo01, lo23, 0x5410) | (uint64_t)(top01 & 0xFFFFu) << 32;
+    codes[1] = (uint64_t)__byte_perm(lo01, lo23, 0x7632) | (uint64_t)(top01 >> 16) << 32;
+    codes[2] = (uint64_t)__byte_perm(hi01, hi23, 0x5410) | (uint64_t)(top23 & 0xFFFFu) << 32;
+    codes[3] = (uint64_t)__byte_perm(hi01, hi23, 0x7632) | (uint64_t)(top23 >> 16) << 32;
+}
+
+// The census of a tile of kCensus4X x ROWS pixels with census4: THREADS
+// threads, each 4 pixels of a row at a time; `tile` holds the window of
+// (kCensus4X + 8) x (ROWS + 6) bytes (census4_tile_bytes).
+constexpr int kCensus4X = 128;
+__host__ __device__ constexpr int census4_tile_bytes(int rows) { return (rows + 6) * (kCensus4X + 8); }
+
+// Copies rows y0 - 3 .. of `image` (clamped), columns x0 - 4 .. x0 - 4 + pitch - 1
+// (clamped), into `window` ([rows][pitch]): every thread's loads first, in
+// flight together (at most MAX_PER a thread), then the shared stores.
+template <int THREADS, int MAX_PER>
+__device__ __forceinline__ void stage_window(const uint8_t *__restrict__ image, int width,
+                                             int height, int x0, int y0, int rows, int pitch,
+                                             uint8_t *window, int tid) {
+    const int cells = rows * pitch;
+    uint8_t v[MAX_PER];
+#pragma unroll
+    for (int k = 0; k < MAX_PER; ++k) {
+        const int i = tid + k * THREADS;
+        if (i < cells) {
+            const int sy = min(max(y0 + i / pitch - 3, 0), height - 1);
+            const int sx = min(max(x0 + i % pitch - 4, 0), width - 1);
+            v[k] = __ldg(image + (size_t)sy * width + sx);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < MAX_PER; ++k) {
+        const int i = tid + k * THREADS;
+        if (i < cells) window[i] = v[k];
+    }
+}
 
 template <int ROWS, int THREADS>
-__device__ __forceinline__ void census_tile(const uint8_t *__restrict__ image, int width,
-                                            int height, uint64_t *__restrict__ codes, int x0,
-                                            int y0, int tid, uint8_t *tile) {
-    constexpr int PITCH = kCensusX + 8;
-    for (int i = tid; i < (ROWS + 6) * PITCH; i += THREADS) {
-        int ty = i / PITCH, tx = i % PITCH;
-        int sy = min(max(y0 + ty - 3, 0), height - 1);
-        int sx = min(max(x0 + tx - 4, 0), width - 1);
-        tile[i] = image[(size_t)sy * width + sx];
-    }
+__device__ __forceinline__ void census4_tile(const uint8_t *__restrict__ image, int width,
+                                             int height, uint64_t *__restrict__ codes, int x0,
+                                             int y0, int tid, uint8_t *tile) {
+    constexpr int PITCH = kCensus4X + 8;
+    stage_window<THREADS, ((ROWS + 6) * PITCH + THREADS - 1) / THREADS>(
+        image, width, height, x0, y0, ROWS + 6, PITCH, tile, tid);
     __syncthreads();
-#pragma unroll
-    for (int i = tid; i < kCensusX * ROWS; i += THREADS) {
-        const int tx = i % kCensusX, ty = i / kCensusX;
+    for (int g = tid; g < (kCensus4X / 4) * ROWS; g += THREADS) {
+        const int tx = 4 * (g % (kCensus4X / 4)), ty = g / (kCensus4X / 4);
         const int x = x0 + tx, y = y0 + ty;
         if (x >= width || y >= height) continue;
-        const uint8_t *centre_at = tile + (ty + 3) * PITCH + tx + 4;
-        const int centre = *centre_at;
-        uint64_t code = 0;
-        int bit = 0;
+        uint64_t four[4];
+        census4(tile, PITCH, tx + 4, ty + 3, four);
+        uint64_t *out = codes + (size_t)y * width + x;
 #pragma unroll
-        for (int dy = -3; dy <= 3; ++dy) {
-            if (dy == 0) continue;
-#pragma unroll
-            for (int dx = -4; dx <= 4; ++dx) {
-                if (dx == 0) continue;
-                int n = centre_at[dy * PITCH + dx];
-                code |= (uint64_t)(n + 1 < centre) << bit;
-                ++bit;
-            }
-        }
-        codes[(size_t)y * width + x] = code;
+        for (int i = 0; i < 4; ++i)
+            if (x + i < width) out[i] = four[i];
     }
 }
 
@@ -87,24 +147,17 @@ __host__ __device__ inline size_t costs_shared_bytes(int disparities) {
            (size_t)kCostPixels * (disparities + 16);
 }
 
-template <int SPAN = 0>
-__device__ __forceinline__ void costs_tile(const uint64_t *__restrict__ left_codes,
-                                           const uint64_t *__restrict__ right_codes, int width,
-                                           int disparities, uint8_t *__restrict__ costs, int x0,
-                                           int y, uint8_t *staged) {
+// Costs of PIXELS pixels of row y from x0 on, from codes staged in shared
+// memory: lefts[i] the code of x0 + i (0 past the image), rights[i] that of
+// x0 - (D - 1) + i (0 outside it); `tile` takes PIXELS x (D + 16) bytes.
+template <int SPAN, int PIXELS>
+__device__ __forceinline__ void costs_from_codes(const uint64_t *lefts, const uint64_t *rights,
+                                                 int width, int disparities,
+                                                 uint8_t *__restrict__ costs, int x0, int y,
+                                                 uint8_t *tile) {
     const int D = disparities, pitch = D + 16;  // tile row pitch: 16-byte stores spread banks
-    uint64_t *lefts = reinterpret_cast<uint64_t *>(staged);
-    uint64_t *rights = lefts + kCostPixels;
-    uint8_t *tile = staged + sizeof(uint64_t) * (2 * kCostPixels + D);
     const size_t row = (size_t)y * width;
-    for (int i = threadIdx.x; i < kCostPixels; i += blockDim.x)
-        lefts[i] = x0 + i < width ? __ldcg(left_codes + row + x0 + i) : 0;
-    for (int i = threadIdx.x; i < kCostPixels + D - 1; i += blockDim.x) {
-        const int x = x0 - (D - 1) + i;
-        rights[i] = (x >= 0 && x < width) ? __ldcg(right_codes + row + x) : 0;
-    }
-    __syncthreads();
-    const int groups = kCostPixels / 4, chunks = D / 16;
+    const int groups = PIXELS / 4, chunks = D / 16;
     for (int t = threadIdx.x; t < groups * chunks; t += blockDim.x) {
         const int p0 = 4 * (t % groups), d0 = 16 * (t / groups);
         // pixel p0 + i at disparity d0 + k reads rights[p0 + i - d0 - k + D - 1]
@@ -132,10 +185,30 @@ __device__ __forceinline__ void costs_tile(const uint64_t *__restrict__ left_cod
         }
     }
     __syncthreads();
-    const int pixels = min(kCostPixels, width - x0);
+    const int pixels = min(PIXELS, width - x0);
     uint4 *out = reinterpret_cast<uint4 *>(costs + (row + x0) * D);
     for (int c = threadIdx.x; c < pixels * chunks; c += blockDim.x)
         out[c] = *reinterpret_cast<const uint4 *>(tile + (c / chunks) * pitch + (c % chunks) * 16);
+}
+
+template <int SPAN = 0>
+__device__ __forceinline__ void costs_tile(const uint64_t *__restrict__ left_codes,
+                                           const uint64_t *__restrict__ right_codes, int width,
+                                           int disparities, uint8_t *__restrict__ costs, int x0,
+                                           int y, uint8_t *staged) {
+    const int D = disparities;
+    uint64_t *lefts = reinterpret_cast<uint64_t *>(staged);
+    uint64_t *rights = lefts + kCostPixels;
+    uint8_t *tile = staged + sizeof(uint64_t) * (2 * kCostPixels + D);
+    const size_t row = (size_t)y * width;
+    for (int i = threadIdx.x; i < kCostPixels; i += blockDim.x)
+        lefts[i] = x0 + i < width ? __ldcg(left_codes + row + x0 + i) : 0;
+    for (int i = threadIdx.x; i < kCostPixels + D - 1; i += blockDim.x) {
+        const int x = x0 - (D - 1) + i;
+        rights[i] = (x >= 0 && x < width) ? __ldcg(right_codes + row + x) : 0;
+    }
+    __syncthreads();
+    costs_from_codes<SPAN, kCostPixels>(lefts, rights, width, D, costs, x0, y, tile);
 }
 
 // ---------------------------------------------------------------- paths

@@ -58,8 +58,8 @@ def test_every_tuning_keeps_the_order(tuning):
 def test_item_counts_follow_the_shapes():
     shapes = [(728, 544, {"disparities": 128}), (97, 31, {"disparities": 64, "paths": 3})]
     items, _, _ = batch.queue(shapes, {"cost_rows": 2, "select_passes": 8})
-    # census: 32 x 16 tiles of both images
-    assert items[0, 0] == 2 * 23 * 34 and items[1, 0] == 2 * 4 * 2
+    # census: 128 x 4 tiles of both images
+    assert items[0, 0] == 2 * 6 * 136 and items[1, 0] == 2 * 1 * 8
     # costs: 64-pixel blocks of 2 rows
     assert items[0, 1] == 12 * 272 and items[1, 1] == 2 * 16
     # selection: 128 / lanes pixels a pass, 8 passes an item (8 lanes at 128 d)
