@@ -327,38 +327,65 @@ __global__ void __launch_bounds__(256)
     uint32_t *right = band;                                     // [ROWS][width]
     float *checked = reinterpret_cast<float *>(band + ROWS * width);  // [ROWS][width]
     const int y0 = blockIdx.x * kBandRows;
-    const int cells = ROWS * width;
-    for (int i = threadIdx.x; i < cells; i += blockDim.x) right[i] = kInvalidKey;
+    for (int i = threadIdx.x; i < ROWS * width; i += blockDim.x) right[i] = kInvalidKey;
     __syncthreads();
-    for (int i = threadIdx.x; i < cells; i += blockDim.x) {
-        const int r = i / width, x = i % width;
-        const int y = min(max(y0 - 1 + r, 0), height - 1);
-        const uint32_t key = __ldcg(keys + (size_t)y * width + x);
-        if (key == kInvalidKey) continue;
-        const int winner = (int)(key & 0xFFFFu);
-        if (x - winner < 0) continue;  // a winner is at most x (past-edge costs lose)
-        atomicMin(&right[r * width + x - winner], (key & 0xFFFF0000u) | (65535u - (uint32_t)winner));
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < cells; i += blockDim.x) {
-        const int r = i / width, x = i % width;
-        const int y = min(max(y0 - 1 + r, 0), height - 1);
-        checked[i] = consistent_value<false>(__ldcg(disparity + (size_t)y * width + x), x, width,
-                                             right + r * width);
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < kBandRows * width; i += blockDim.x) {
-        const int ry = i / width, x = i % width, y = y0 + ry;
-        if (y >= height) break;
-        float v[9];
+    // Keys into the right maps, the disparities kept raw in `checked`: the
+    // loads of kCheckChunk columns of every row a thread are issued together,
+    // then used. Loops run over rows and columns (no division by the width).
+    constexpr int kCheckChunk = 3;
+    for (int xb = threadIdx.x; xb < width; xb += kCheckChunk * blockDim.x) {
+        uint32_t key[ROWS][kCheckChunk];
+        float value[ROWS][kCheckChunk];
 #pragma unroll
-        for (int dy = -1; dy <= 1; ++dy)
+        for (int r = 0; r < ROWS; ++r) {
+            const size_t row = (size_t)min(max(y0 - 1 + r, 0), height - 1) * width;
 #pragma unroll
-            for (int dx = -1; dx <= 1; ++dx) {
-                const int sx = min(max(x + dx, 0), width - 1);
-                v[(dy + 1) * 3 + dx + 1] = checked[(ry + 1 + dy) * width + sx];
+            for (int k = 0; k < kCheckChunk; ++k) {
+                const int x = xb + k * blockDim.x;
+                if (x < width) {
+                    key[r][k] = __ldcg(keys + row + x);
+                    value[r][k] = __ldcg(disparity + row + x);
+                }
             }
-        filtered[(size_t)y * width + x] = median_of_nine(v, stage_mask);
+        }
+#pragma unroll
+        for (int r = 0; r < ROWS; ++r) {
+#pragma unroll
+            for (int k = 0; k < kCheckChunk; ++k) {
+                const int x = xb + k * blockDim.x;
+                if (x >= width) continue;
+                checked[r * width + x] = value[r][k];
+                const uint32_t found = key[r][k];
+                if (found == kInvalidKey) continue;
+                const int winner = (int)(found & 0xFFFFu);
+                if (x - winner < 0) continue;  // a winner is at most x (past-edge costs lose)
+                atomicMin(&right[r * width + x - winner],
+                          (found & 0xFFFF0000u) | (65535u - (uint32_t)winner));
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r)
+        for (int x = threadIdx.x; x < width; x += blockDim.x)
+            checked[r * width + x] =
+                consistent_value<false>(checked[r * width + x], x, width, right + r * width);
+    __syncthreads();
+#pragma unroll
+    for (int ry = 0; ry < kBandRows; ++ry) {
+        const int y = y0 + ry;
+        if (y >= height) break;
+        for (int x = threadIdx.x; x < width; x += blockDim.x) {
+            float v[9];
+#pragma unroll
+            for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int sx = min(max(x + dx, 0), width - 1);
+                    v[(dy + 1) * 3 + dx + 1] = checked[(ry + 1 + dy) * width + sx];
+                }
+            filtered[(size_t)y * width + x] = median_of_nine(v, stage_mask);
+        }
     }
 }
 

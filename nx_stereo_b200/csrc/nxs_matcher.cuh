@@ -576,7 +576,9 @@ __device__ __forceinline__ void select_pixels(const void *__restrict__ source, i
     const bool valid = pixel < (size_t)width * height;
     const int D = disparities;
     const bool active = valid && member * 16 < D;
-    const int x = valid ? (int)(pixel % width) : 0;
+    // A 32-bit remainder: pixel < 2^32, as 2^32 pixels' volumes (at least
+    // 16 bytes a pixel) would not fit in device memory.
+    const int x = valid ? (int)((uint32_t)pixel % (uint32_t)width) : 0;
     const int d0 = member * 16;
     uint32_t v[8];
 #pragma unroll

@@ -151,9 +151,94 @@ __global__ void __launch_bounds__(kSpeckleX *kSpeckleY)
     despeckled[(size_t)y * width + x] = kept ? centre : -1.0f;
 }
 
+// The same filter with the radius fixed at compile time: a thread takes
+// kSpeckleRun pixels down a column, so each window row it reads from shared
+// memory (2R + 1 values, into registers) serves every one of its pixels whose
+// window holds it: (kSpeckleRun + 2R) x (2R + 1) shared loads for
+// kSpeckleRun x ((2R + 1)^2 - 1) comparisons. The window's global loads are
+// all issued before any is stored.
+constexpr int kSpeckleRun = 4;
+
+template <int R>
+__global__ void __launch_bounds__(kSpeckleX *kSpeckleY)
+    despeckle_run_kernel(const float *__restrict__ disparity, int width, int height,
+                         float min_support, float max_diff, float *__restrict__ despeckled) {
+    constexpr int TW = kSpeckleX + 2 * R, TH = kSpeckleY * kSpeckleRun + 2 * R;
+    constexpr int THREADS = kSpeckleX * kSpeckleY, PER = (TW * TH + THREADS - 1) / THREADS;
+    __shared__ float window[TH][TW];
+    follow_previous_grid();
+    const int x0 = blockIdx.x * kSpeckleX, y0 = blockIdx.y * kSpeckleY * kSpeckleRun;
+    const int tid = threadIdx.y * kSpeckleX + threadIdx.x;
+    float v[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int i = tid + k * THREADS;
+        if (i < TW * TH) {
+            const int sy = y0 + i / TW - R, sx = x0 + i % TW - R;
+            v[k] = (sy >= 0 && sy < height && sx >= 0 && sx < width)
+                       ? disparity[(size_t)sy * width + sx]
+                       : -1.0f;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int i = tid + k * THREADS;
+        if (i < TW * TH) window[i / TW][i % TW] = v[k];
+    }
+    __syncthreads();
+    const int tx = threadIdx.x, top = threadIdx.y * kSpeckleRun;  // the run's first window row - R
+    float centre[kSpeckleRun];
+    unsigned support[kSpeckleRun];
+#pragma unroll
+    for (int k = 0; k < kSpeckleRun; ++k) {
+        centre[k] = window[top + k + R][tx + R];
+        support[k] = 0;
+    }
+#pragma unroll
+    for (int r = 0; r < kSpeckleRun + 2 * R; ++r) {
+        float row[2 * R + 1];
+#pragma unroll
+        for (int dx = 0; dx <= 2 * R; ++dx) row[dx] = window[top + r][tx + dx];
+#pragma unroll
+        for (int k = 0; k < kSpeckleRun; ++k) {
+            const int dy = r - k;  // the row's place in pixel k's window
+            if (dy < 0 || dy > 2 * R) continue;
+#pragma unroll
+            for (int dx = 0; dx <= 2 * R; ++dx) {
+                if (dy == R && dx == R) continue;
+                const float n = row[dx];
+                support[k] += (n > 0.0f) & (fabsf(fsub(n, centre[k])) <= max_diff);
+            }
+        }
+    }
+    const int x = x0 + tx;
+#pragma unroll
+    for (int k = 0; k < kSpeckleRun; ++k) {
+        const int y = y0 + top + k;
+        if (x < width && y < height) {
+            const bool kept = centre[k] > 0.0f && (float)support[k] >= min_support;
+            despeckled[(size_t)y * width + x] = kept ? centre[k] : -1.0f;
+        }
+    }
+}
+
 cudaError_t launch_despeckle(const float *disparity, int width, int height, float min_support,
                              float max_diff, int radius, float *despeckled, cudaStream_t stream) {
     dim3 block(kSpeckleX, kSpeckleY);
+    dim3 runs((width + kSpeckleX - 1) / kSpeckleX,
+              (height + kSpeckleY * kSpeckleRun - 1) / (kSpeckleY * kSpeckleRun));
+#define NXS_DESPECKLE(R)                                                                      \
+    return launch_after(despeckle_run_kernel<R>, runs, block, 0, stream, disparity, width,    \
+                        height, min_support, max_diff, despeckled)
+    switch (radius) {
+    case 1: NXS_DESPECKLE(1);
+    case 2: NXS_DESPECKLE(2);
+    case 3: NXS_DESPECKLE(3);
+    case 4: NXS_DESPECKLE(4);
+    case 5: NXS_DESPECKLE(5);
+    default: break;
+    }
+#undef NXS_DESPECKLE
     dim3 grid((width + kSpeckleX - 1) / kSpeckleX, (height + kSpeckleY - 1) / kSpeckleY);
     size_t shared = sizeof(float) * (kSpeckleX + 2 * radius) * (kSpeckleY + 2 * radius);
     return launch_after(despeckle_kernel, grid, block, shared, stream, disparity, width, height,

@@ -89,10 +89,12 @@ def random_disparity(rng, h, w):
     return d
 
 
-@pytest.mark.parametrize("radius", [1, 3, 5])
-def test_despeckle_is_bit_exact(native, oracle, radius):
+# Radii 1-5 run the kernel with the radius compiled in, 6-8 the general one.
+@pytest.mark.parametrize("radius", [1, 2, 3, 4, 5, 6, 8])
+@pytest.mark.parametrize("size", [(97, 131), (33, 1), (1, 40), (128, 64)])
+def test_despeckle_is_bit_exact(native, oracle, radius, size):
     rng = np.random.default_rng(radius)
-    d = random_disparity(rng, 97, 131)
+    d = random_disparity(rng, *size)
     for min_support, max_diff in [(12, 1.0), (0, 1.0), (3, 0.25), (24, 8.0)]:
         want = oracle.despeckle(d, min_support, max_diff, radius)
         assert g.same_bits(despeckle_gpu(native, d, min_support, max_diff, radius), want)
