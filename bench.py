@@ -39,7 +39,7 @@ import numpy as np  # noqa: E402
 METRIC = "pairs/s at 728x544x128 d, 8 paths (full frame-to-depth pipeline)"
 WIDTH, HEIGHT, DISPARITIES, PATHS = 728, 544, 128, 8
 DECIMATION = 4
-KERNELS_PER_STEP = 9  # rectify, census, costs, paths, select, check+median, despeckle, depth, cloud
+KERNELS_PER_STEP = 8  # rectify, census+costs, paths, select, check+median, despeckle, depth, cloud
 PATHS_EVERY = 4  # timed steps between those whose path kernel is bracketed by events
 # At most this many pairs on the device at once in the serving run, oldest
 # arrival first (None: up to every stream's request slots; caps of 4, 8 and 16
@@ -161,7 +161,6 @@ class DevicePipeline:
         dev = torch.device("cuda")
         u8, f32 = torch.uint8, torch.float32
         self.images = torch.empty((2, HEIGHT, WIDTH), dtype=u8, device=dev)
-        self.codes = torch.empty((2, HEIGHT, WIDTH), dtype=torch.int64, device=dev)
         self.costs = torch.empty(vol, dtype=u8, device=dev)
         self.volumes = torch.empty(PATHS * vol, dtype=u8, device=dev)
         self.selected = torch.empty(px, dtype=f32, device=dev)
@@ -177,8 +176,8 @@ class DevicePipeline:
         # The costs and path volumes in the order the matcher itself keeps them.
         self.span = int(native.load().nxs_matcher_span(DISPARITIES))
 
-    STAGES = ["rectify", "census", "costs", "paths", "select", "check_median",
-              "despeckle", "depth", "cloud"]
+    STAGES = ["rectify", "census_costs", "paths", "select", "check_median", "despeckle",
+              "depth", "cloud"]
 
     def step(self, frames, marks=None):
         """One pair; `marks` (len(STAGES) + 1 CUDA events or None) bracket the
@@ -198,31 +197,29 @@ class DevicePipeline:
              HEIGHT, ctypes.byref(self.cameras[0]), ctypes.byref(self.cameras[1]), WIDTH, HEIGHT,
              self.images[0].data_ptr(), self.images[1].data_ptr(), s)
         mark(1)
-        call("nxs_census_pair_device", self.images[0].data_ptr(), self.images[1].data_ptr(),
-             WIDTH, HEIGHT, self.codes[0].data_ptr(), self.codes[1].data_ptr(), s)
+        call("nxs_census_costs_device_ordered", self.images[0].data_ptr(),
+             self.images[1].data_ptr(), WIDTH, HEIGHT, DISPARITIES, self.span,
+             self.costs.data_ptr(), s)
         mark(2)
-        call("nxs_costs_device_ordered", self.codes[0].data_ptr(), self.codes[1].data_ptr(), WIDTH,
-             HEIGHT, DISPARITIES, self.span, self.costs.data_ptr(), s)
-        mark(3)
         call("nxs_paths_device_ordered", self.costs.data_ptr(), WIDTH, HEIGHT, DISPARITIES, PATHS,
              8, 64, self.span, self.volumes.data_ptr(), s)
-        mark(4)
+        mark(3)
         call("nxs_select_paths_device_ordered", self.volumes.data_ptr(), WIDTH, HEIGHT,
              DISPARITIES, PATHS, 1.0526315789473684, self.span, self.selected.data_ptr(),
              self.keys.data_ptr(), s)
-        mark(5)
+        mark(4)
         call("nxs_check_median_device", self.selected.data_ptr(), self.keys.data_ptr(), WIDTH,
              HEIGHT, 1, self.disparity.data_ptr(), s)
-        mark(6)
+        mark(5)
         call("nxs_despeckle_device", self.disparity.data_ptr(), WIDTH, HEIGHT, 12.0, 1.0, 3,
              self.speckled.data_ptr(), s)
-        mark(7)
+        mark(6)
         call("nxs_depth_device", self.speckled.data_ptr(), WIDTH * HEIGHT, self.focal,
              self.baseline, self.depth_mm.data_ptr(), self.depth_m.data_ptr(), s)
-        mark(8)
+        mark(7)
         call("nxs_cloud_device", self.depth_m.data_ptr(), WIDTH, HEIGHT, DECIMATION, self.focal,
              self.cx, self.cy, 0.05, 20.0, self.grid.data_ptr(), self.kept.data_ptr(), s)
-        mark(9)
+        mark(8)
 
 
 def run_ours(args, rank, world, local_rank):

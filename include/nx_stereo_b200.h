@@ -280,6 +280,13 @@ uint32_t nxs_matcher_span(uint32_t disparities);
 nxs_status nxs_costs_device_ordered(const uint64_t *d_left_codes, const uint64_t *d_right_codes,
                                     uint32_t width, uint32_t height, uint32_t disparities,
                                     uint32_t span, uint8_t *d_costs, void *stream);
+/* The census of both u8 images and the cost volume in one launch, the codes
+ * kept in shared memory: the costs nxs_census_pair_device followed by
+ * nxs_costs_device_ordered give (lib/nx_stereo.ex:491-542), in the order of
+ * `span`; this is the first step nxs_sgm runs. */
+nxs_status nxs_census_costs_device_ordered(const uint8_t *d_left, const uint8_t *d_right,
+                                           uint32_t width, uint32_t height, uint32_t disparities,
+                                           uint32_t span, uint8_t *d_costs, void *stream);
 nxs_status nxs_paths_device_ordered(const uint8_t *d_costs, uint32_t width, uint32_t height,
                                     uint32_t disparities, uint32_t paths, uint32_t p1, uint32_t p2,
                                     uint32_t span, uint8_t *d_paths, void *stream);

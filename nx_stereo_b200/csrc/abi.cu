@@ -115,6 +115,36 @@ struct PinnedPool {
     std::map<void *, size_t> sizes;
 };
 
+// The events of finished requests, kept for the next ones, so that a request
+// neither creates nor destroys events (one per member boundary and one for
+// done). A request gives its events back only after its done event, which
+// follows every one of them, has completed.
+struct EventPool {
+    std::mutex lock;
+    std::vector<cudaEvent_t> timed, untimed;
+    cudaError_t take(bool timing, cudaEvent_t *ev) {
+        {
+            std::lock_guard<std::mutex> g(lock);
+            std::vector<cudaEvent_t> &free_events = timing ? timed : untimed;
+            if (!free_events.empty()) {
+                *ev = free_events.back();
+                free_events.pop_back();
+                return cudaSuccess;
+            }
+        }
+        return timing ? cudaEventCreate(ev) : cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+    }
+    void give(bool timing, cudaEvent_t ev) {
+        if (!ev) return;
+        std::lock_guard<std::mutex> g(lock);
+        (timing ? timed : untimed).push_back(ev);
+    }
+    ~EventPool() {
+        for (cudaEvent_t ev : timed) cudaEventDestroy(ev);
+        for (cudaEvent_t ev : untimed) cudaEventDestroy(ev);
+    }
+};
+
 enum class Kind { Rectification, Disparity, Speckle, Temporal, Depth, Cloud, Quality };
 
 struct Member {
@@ -165,6 +195,7 @@ struct Segment {
     std::mutex order;  // one request enqueued at a time
     uint64_t sequence = 0;
     PinnedPool pinned;
+    EventPool events;
     Slot slots[kSlots];
     // shared by every request, touched only on `stream`
     float *depth_m = nullptr, *quality_columns = nullptr;
@@ -482,6 +513,20 @@ extern "C" nxs_status nxs_costs_device_ordered(const uint64_t *d_left_codes,
                (span == 0 || span == 8 || span == 16));
     return launch_costs(d_left_codes, d_right_codes, width, height, disparities, d_costs,
                         static_cast<cudaStream_t>(stream), (int)span)
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_census_costs_device_ordered(const uint8_t *d_left,
+                                                      const uint8_t *d_right, uint32_t width,
+                                                      uint32_t height, uint32_t disparities,
+                                                      uint32_t span, uint8_t *d_costs,
+                                                      void *stream) {
+    CHECK_SIZE(d_left && d_right && d_costs && width > 0 && height > 0 &&
+               disparities % 16 == 0 && disparities >= 16 && disparities <= 256 &&
+               (span == 0 || span == 8 || span == 16));
+    return launch_census_costs(d_left, d_right, width, height, disparities, d_costs,
+                               static_cast<cudaStream_t>(stream), (int)span)
                ? NXS_CUDA_ERROR
                : NXS_OK;
 }
@@ -1122,8 +1167,8 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
     cudaError_t e = cudaSuccess;
     const size_t n = seg->members.size();
     r->marks.resize(n + 1, nullptr);
-    for (size_t i = 0; i <= n && !e; ++i) e = cudaEventCreate(&r->marks[i]);
-    if (!e) e = cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming);
+    for (size_t i = 0; i <= n && !e; ++i) e = seg->events.take(true, &r->marks[i]);
+    if (!e) e = seg->events.take(false, &r->done);
     // Stage the entries in pinned memory now: the caller's buffers are only
     // borrowed for the call.
     std::vector<void *> staged(seg->entries.size(), nullptr);
@@ -1322,9 +1367,8 @@ extern "C" void nxs_request_free(nxs_request *r) {
     if (!r) return;
     cudaSetDevice(r->segment->device);
     if (r->done) cudaEventSynchronize(r->done);
-    for (cudaEvent_t ev : r->marks)
-        if (ev) cudaEventDestroy(ev);
-    if (r->done) cudaEventDestroy(r->done);
+    for (cudaEvent_t ev : r->marks) r->segment->events.give(true, ev);
+    r->segment->events.give(false, r->done);
     for (void *p : r->pinned) r->segment->pinned.give(p);
     delete r;
 }

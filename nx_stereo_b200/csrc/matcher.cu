@@ -70,6 +70,35 @@ cudaError_t launch_costs(const uint64_t *left_codes, const uint64_t *right_codes
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------- census + costs
+// A block of 128 threads takes kCensusCostPixels pixels of one row: the
+// census of both images around them and their costs (census_costs_tile).
+template <int SPAN>
+__global__ void __launch_bounds__(128)
+    census_costs_kernel(const uint8_t *__restrict__ left, const uint8_t *__restrict__ right,
+                        int width, int height, int disparities, uint8_t *__restrict__ costs) {
+    follow_previous_grid();
+    extern __shared__ __align__(16) uint8_t staged[];
+    census_costs_tile<SPAN, kCensusCostPixels, 128>(left, right, width, height, disparities,
+                                                    costs, blockIdx.x * kCensusCostPixels,
+                                                    blockIdx.y, staged, threadIdx.x);
+}
+
+cudaError_t launch_census_costs(const uint8_t *left, const uint8_t *right, int width, int height,
+                                int disparities, uint8_t *costs, cudaStream_t stream, int span) {
+    if (disparities < 16 || disparities > 256 || disparities % 16) return cudaErrorInvalidValue;
+    dim3 grid((width + kCensusCostPixels - 1) / kCensusCostPixels, height);
+    const size_t shared = census_costs_shared_bytes(kCensusCostPixels, disparities);
+#define NXS_CENSUS_COSTS(S)                                                                   \
+    launch_after(census_costs_kernel<S>, grid, dim3(128), shared, stream, left, right, width, \
+                 height, disparities, costs)
+    if (span == 16) NXS_CENSUS_COSTS(16);
+    else if (span == 8) NXS_CENSUS_COSTS(8);
+    else NXS_CENSUS_COSTS(0);
+#undef NXS_CENSUS_COSTS
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------- paths
 // One warp per block, so blocks go to SMs as they free up, longest lines first.
 template <int G, int WORDS, bool FULL, int SPAN>
@@ -437,13 +466,10 @@ cudaError_t run_matcher(const uint8_t *left, const uint8_t *right, int width, in
                         int stage_mask, const MatcherScratch &s, float *disparity,
                         cudaStream_t stream) {
     cudaError_t e;
-    if ((e = launch_census(left, right, width, height, s.left_codes, s.right_codes, stream)))
-        return e;
     // The intermediates are in the permuted order of the path lanes' span
     // (span_disparity).
     const int span = matcher_span(disparities);
-    if ((e = launch_costs(s.left_codes, s.right_codes, width, height, disparities, s.costs,
-                          stream, span)))
+    if ((e = launch_census_costs(left, right, width, height, disparities, s.costs, stream, span)))
         return e;
     if ((e = launch_paths(s.costs, width, height, disparities, paths, p1, p2, s.paths, stream,
                           span)))

@@ -31,6 +31,11 @@ cudaError_t launch_census(const uint8_t *left, const uint8_t *right, int width, 
 cudaError_t launch_costs(const uint64_t *left_codes, const uint64_t *right_codes, int width,
                          int height, int disparities, uint8_t *costs, cudaStream_t stream,
                          int span = 0);
+// The census of both images and the costs in one launch (the codes stay in
+// shared memory): the same costs as launch_census then launch_costs.
+cudaError_t launch_census_costs(const uint8_t *left, const uint8_t *right, int width, int height,
+                                int disparities, uint8_t *costs, cudaStream_t stream,
+                                int span = 0);
 // paths_out[p][y][x][d] (u8) for p < paths; span 8 or 16: costs and path
 // costs in that permuted order (span 0: natural).
 cudaError_t launch_paths(const uint8_t *costs, int width, int height, int disparities, int paths,

@@ -97,6 +97,43 @@ __device__ __forceinline__ void stage_window(const uint8_t *__restrict__ image, 
     }
 }
 
+// stage_window for a pitch known only at run time (at most MAX_PITCH): ROWS
+// rows, each thread columns tid, tid + THREADS, ... of every row, all loads
+// in flight together, with no division by the pitch.
+template <int THREADS, int ROWS, int MAX_PITCH>
+__device__ __forceinline__ void stage_rows(const uint8_t *__restrict__ image, int width,
+                                           int height, int x0, int y0, int pitch,
+                                           uint8_t *window, int tid) {
+    constexpr int PER_ROW = (MAX_PITCH + THREADS - 1) / THREADS;
+    uint8_t v[ROWS][PER_ROW];
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r) {
+        const uint8_t *row = image + (size_t)min(max(y0 + r - 3, 0), height - 1) * width;
+#pragma unroll
+        for (int k = 0; k < PER_ROW; ++k) {
+            const int c = tid + k * THREADS;
+            if (c < pitch) v[r][k] = __ldg(row + min(max(x0 + c - 4, 0), width - 1));
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r)
+#pragma unroll
+        for (int k = 0; k < PER_ROW; ++k) {
+            const int c = tid + k * THREADS;
+            if (c < pitch) window[r * pitch + c] = v[r][k];
+        }
+}
+
+// n / d for 0 <= n < 2^16 and 0 < d <= 16 by a multiply-high of 16 n with
+// magic = 0x0FFFFFFF / d + 1 (ceil(2^28 / d), which fits 32 bits for every d
+// including 1): the rounding error 16 n / 2^32 stays below 1 / d.
+__host__ __device__ constexpr uint32_t small_divisor_magic(uint32_t d) {
+    return 0x0FFFFFFFu / d + 1u;
+}
+__device__ __forceinline__ uint32_t divide_small(uint32_t n, uint32_t magic) {
+    return __umulhi(n << 4, magic);
+}
+
 template <int ROWS, int THREADS>
 __device__ __forceinline__ void census4_tile(const uint8_t *__restrict__ image, int width,
                                              int height, uint64_t *__restrict__ codes, int x0,
@@ -123,10 +160,11 @@ __device__ __forceinline__ void census4_tile(const uint8_t *__restrict__ image, 
 // the image zero (lib/nx_stereo.ex:528-542). SPAN 8 or 16 stores each run of
 // SPAN disparities in the permuted order of span_disparity, the order the
 // matcher's own path and selection kernels work in. A block of 128 threads covers 64
-// pixels of a row. It stages their left codes and the D + 63 right codes they
-// reach; a thread computes 4 neighbouring pixels x 16 disparities, whose right
-// codes are 19 consecutive ones held in registers, into a shared tile, and the
-// block then writes its 64 x D bytes out contiguously with 16-byte stores.
+// pixels of a row. It stages their left codes and the D + 64 right codes from
+// x0 - D on; a thread computes 4 neighbouring pixels x 16 disparities, whose
+// right codes are 19 consecutive ones held in registers, into a shared tile,
+// and the block then writes its 64 x D bytes out contiguously with 16-byte
+// stores.
 constexpr int kCostPixels = 64;
 
 // The permuted disparity order: within each run of SPAN disparities, bytes 2k
@@ -143,52 +181,78 @@ __host__ __device__ constexpr int span_position(int span, int d) {
 }
 
 __host__ __device__ inline size_t costs_shared_bytes(int disparities) {
-    return sizeof(uint64_t) * (2 * kCostPixels + disparities) +
-           (size_t)kCostPixels * (disparities + 16);
+    return sizeof(uint64_t) * (2 * kCostPixels + disparities) + (size_t)kCostPixels * disparities;
 }
 
 // Costs of PIXELS pixels of row y from x0 on, from codes staged in shared
-// memory: lefts[i] the code of x0 + i (0 past the image), rights[i] that of
-// x0 - (D - 1) + i (0 outside it); `tile` takes PIXELS x (D + 16) bytes.
+// memory (16-byte aligned): lefts[i] the code of x0 + i (0 past the image),
+// rights[i] that of x0 - D + i (0 outside it), PIXELS + D of them; `tile`
+// (16-byte aligned) takes PIXELS x D bytes.
+//
+// Shared-memory banks: a warp's threads take 32 neighbouring groups of 4
+// pixels at one run of 16 disparities. Their code windows start 4 codes (32
+// bytes) apart and are read as 16-byte pairs, so a read serves 4 threads per
+// 128 bytes. Each tile row is D bytes with its 16-byte runs rotated by the
+// pixel's group (run q of pixel p at (q + p / 4) mod D / 16), so a warp's
+// 16-byte stores to four pixel rows fall in 8 different bank quads; the
+// write-out undoes the rotation.
 template <int SPAN, int PIXELS>
 __device__ __forceinline__ void costs_from_codes(const uint64_t *lefts, const uint64_t *rights,
                                                  int width, int disparities,
                                                  uint8_t *__restrict__ costs, int x0, int y,
                                                  uint8_t *tile) {
-    const int D = disparities, pitch = D + 16;  // tile row pitch: 16-byte stores spread banks
+    const int D = disparities;
     const size_t row = (size_t)y * width;
     const int groups = PIXELS / 4, chunks = D / 16;
+    const uint32_t magic = small_divisor_magic((uint32_t)chunks);  // divide_small by chunks
     for (int t = threadIdx.x; t < groups * chunks; t += blockDim.x) {
-        const int p0 = 4 * (t % groups), d0 = 16 * (t / groups);
-        // pixel p0 + i at disparity d0 + k reads rights[p0 + i - d0 - k + D - 1]
-        //                                     = window[i - k + 15]
-        const uint64_t *base = rights + p0 - d0 + D - 16;
-        uint64_t window[19];
+        const int group = t % groups, q = t / groups;
+        const int p0 = 4 * group, d0 = 16 * q;
+        // pixel p0 + i at disparity d0 + k reads rights[p0 + i - d0 - k + D]
+        //   = window[16 + i - k], window[m] = rights[p0 - d0 + D - 16 + m]
+        // (m = 1..19; the first of the 20 is read for the 16-byte alignment)
+        const uint4 *base = reinterpret_cast<const uint4 *>(rights + p0 - d0 + D - 16);
+        uint64_t window[20];
 #pragma unroll
-        for (int j = 0; j < 19; ++j) window[j] = base[j];
+        for (int j = 0; j < 10; ++j) {
+            const uint4 two = base[j];
+            window[2 * j] = (uint64_t)two.x | (uint64_t)two.y << 32;
+            window[2 * j + 1] = (uint64_t)two.z | (uint64_t)two.w << 32;
+        }
+        const uint4 *left_pairs = reinterpret_cast<const uint4 *>(lefts + p0);
+        const uint4 l01 = left_pairs[0], l23 = left_pairs[1];
+        const uint64_t l4[4] = {(uint64_t)l01.x | (uint64_t)l01.y << 32,
+                                (uint64_t)l01.z | (uint64_t)l01.w << 32,
+                                (uint64_t)l23.x | (uint64_t)l23.y << 32,
+                                (uint64_t)l23.z | (uint64_t)l23.w << 32};
+        int rotated = q + group - chunks * (int)divide_small(group, magic);  // q + group % chunks
+        if (rotated >= chunks) rotated -= chunks;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const uint64_t l = lefts[p0 + i];
             uint32_t words[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int w4 = 0; w4 < 4; ++w4) {
                 uint32_t w = 0;
 #pragma unroll
                 for (int b = 0; b < 4; ++b) {
-                    const int k = span_disparity(SPAN, 4 * q + b);
-                    w |= (uint32_t)__popcll(l ^ window[i - k + 15]) << (8 * b);
+                    const int k = span_disparity(SPAN, 4 * w4 + b);
+                    w |= (uint32_t)__popcll(l4[i] ^ window[16 + i - k]) << (8 * b);
                 }
-                words[q] = w;
+                words[w4] = w;
             }
-            *reinterpret_cast<uint4 *>(tile + (p0 + i) * pitch + d0) =
+            *reinterpret_cast<uint4 *>(tile + (p0 + i) * D + 16 * rotated) =
                 make_uint4(words[0], words[1], words[2], words[3]);
         }
     }
     __syncthreads();
     const int pixels = min(PIXELS, width - x0);
     uint4 *out = reinterpret_cast<uint4 *>(costs + (row + x0) * D);
-    for (int c = threadIdx.x; c < pixels * chunks; c += blockDim.x)
-        out[c] = *reinterpret_cast<const uint4 *>(tile + (c / chunks) * pitch + (c % chunks) * 16);
+    for (int c = threadIdx.x; c < pixels * chunks; c += blockDim.x) {
+        const int p = (int)divide_small(c, magic), g = p / 4;
+        int rotated = c - p * chunks + g - chunks * (int)divide_small(g, magic);
+        if (rotated >= chunks) rotated -= chunks;
+        out[c] = *reinterpret_cast<const uint4 *>(tile + p * D + 16 * rotated);
+    }
 }
 
 template <int SPAN = 0>
@@ -203,12 +267,74 @@ __device__ __forceinline__ void costs_tile(const uint64_t *__restrict__ left_cod
     const size_t row = (size_t)y * width;
     for (int i = threadIdx.x; i < kCostPixels; i += blockDim.x)
         lefts[i] = x0 + i < width ? __ldcg(left_codes + row + x0 + i) : 0;
-    for (int i = threadIdx.x; i < kCostPixels + D - 1; i += blockDim.x) {
-        const int x = x0 - (D - 1) + i;
+    for (int i = threadIdx.x; i < kCostPixels + D; i += blockDim.x) {
+        const int x = x0 - D + i;
         rights[i] = (x >= 0 && x < width) ? __ldcg(right_codes + row + x) : 0;
     }
     __syncthreads();
     costs_from_codes<SPAN, kCostPixels>(lefts, rights, width, D, costs, x0, y, tile);
+}
+
+// ---------------------------------------------------------------- census + costs
+// Both steps for PIXELS pixels of row y from x0 on, in one block of THREADS
+// threads: the block stages the 7 rows of both images around row y that the
+// pixels' census windows reach (the left image's columns x0 - 4 .. x0 +
+// PIXELS + 3, the right image's x0 - D - 4 .. x0 + PIXELS + 3, clamped as the
+// census clamps), takes census4 of the PIXELS left pixels and of the PIXELS + D
+// right pixels from x0 - D on into shared memory (0 outside the image), and
+// forms the costs from them with costs_from_codes. The codes never reach
+// global memory; each right code is formed by up to (PIXELS + D) / PIXELS
+// blocks, which is integer work beside the popcounts that bound the costs.
+constexpr int kCensusCostPixels = 128;
+
+__host__ __device__ constexpr int census_costs_window_bytes(int pixels, int disparities) {
+    return (7 * (pixels + 8) + 7 * (pixels + disparities + 8) + 15) / 16 * 16;
+}
+
+__host__ __device__ inline size_t census_costs_shared_bytes(int pixels, int disparities) {
+    return sizeof(uint64_t) * (2 * pixels + disparities) +
+           census_costs_window_bytes(pixels, disparities) + (size_t)pixels * disparities;
+}
+
+template <int SPAN, int PIXELS, int THREADS, int MAX_DISPARITIES = 256>
+__device__ __forceinline__ void census_costs_tile(const uint8_t *__restrict__ left_image,
+                                                  const uint8_t *__restrict__ right_image,
+                                                  int width, int height, int disparities,
+                                                  uint8_t *__restrict__ costs, int x0, int y,
+                                                  uint8_t *staged, int tid) {
+    static_assert(PIXELS % 4 == 0, "census4 takes four pixels at once");
+    const int D = disparities;
+    const int left_pitch = PIXELS + 8, right_pitch = PIXELS + D + 8;
+    uint64_t *lefts = reinterpret_cast<uint64_t *>(staged);   // x0 ..
+    uint64_t *rights = lefts + PIXELS;                         // x0 - D ..
+    uint8_t *left_window = reinterpret_cast<uint8_t *>(rights + PIXELS + D);
+    uint8_t *right_window = left_window + 7 * left_pitch;
+    uint8_t *tile = left_window + census_costs_window_bytes(PIXELS, D);
+    stage_rows<THREADS, 7, PIXELS + 8>(left_image, width, height, x0, y, left_pitch, left_window,
+                                       tid);
+    stage_rows<THREADS, 7, PIXELS + MAX_DISPARITIES + 8>(right_image, width, height, x0 - D, y,
+                                                         right_pitch, right_window, tid);
+    __syncthreads();
+    constexpr int kLeftGroups = PIXELS / 4;
+    const int groups = kLeftGroups + (PIXELS + D) / 4;
+    for (int g = tid; g < groups; g += THREADS) {
+        uint64_t four[4];
+        if (g < kLeftGroups) {
+            census4(left_window, left_pitch, 4 * g + 4, 3, four);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) lefts[4 * g + i] = x0 + 4 * g + i < width ? four[i] : 0;
+        } else {
+            const int r = g - kLeftGroups;
+            census4(right_window, right_pitch, 4 * r + 4, 3, four);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int x = x0 - D + 4 * r + i;
+                rights[4 * r + i] = (x >= 0 && x < width) ? four[i] : 0;
+            }
+        }
+    }
+    __syncthreads();
+    costs_from_codes<SPAN, PIXELS>(lefts, rights, width, D, costs, x0, y, tile);
 }
 
 // ---------------------------------------------------------------- paths

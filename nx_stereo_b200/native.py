@@ -129,6 +129,7 @@ SIGNATURES = {
     "nxs_select_device": (_i, [_P, _u32, _u32, _u32, _f, _P, _P, _P]),
     "nxs_matcher_span": (_u32, [_u32]),
     "nxs_costs_device_ordered": (_i, [_P, _P, _u32, _u32, _u32, _u32, _P, _P]),
+    "nxs_census_costs_device_ordered": (_i, [_P, _P, _u32, _u32, _u32, _u32, _P, _P]),
     "nxs_paths_device_ordered": (_i, [_P, _u32, _u32, _u32, _u32, _u32, _u32, _u32, _P, _P]),
     "nxs_select_paths_device_ordered": (_i, [_P, _u32, _u32, _u32, _u32, _f, _u32, _P, _P, _P]),
     "nxs_consistency_device": (_i, [_P, _P, _u32, _u32, _P, _P]),
@@ -219,6 +220,26 @@ class _PinnedView:
         self._request = request
         self.__array_interface__ = {"data": (address, False), "shape": shape,
                                     "typestr": dtype.str, "version": 3}
+
+
+class PreparedParams:
+    """A segment's per-member live params marshalled once for nxs_run_async
+    (a list of {name: float or sequence}, one per member, names sorted): a
+    segment whose params do not change between pairs reuses it."""
+
+    def __init__(self, params):
+        self.count = len(params)
+        self._keep = []
+        self.members = (MemberParams * max(self.count, 1))()
+        for i, member in enumerate(params):
+            ps = (Param * max(len(member), 1))()
+            for j, (name, value) in enumerate(sorted(member.items())):
+                values = np.ascontiguousarray(np.atleast_1d(np.asarray(value, np.float32)))
+                b = name.encode()
+                self._keep += [b, values]
+                ps[j] = Param(b, values.size, values.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+            self._keep.append(ps)
+            self.members[i] = MemberParams(len(member), ps)
 
 
 class Request:
@@ -335,18 +356,11 @@ class Context:
                                     buf, 1024), buf)
 
     def run_async(self, segment, params, entries, done=None, tag=0):
-        """params: per member {name: float or sequence}; entries: {name: ndarray}."""
-        keep = []
-        mps = (MemberParams * max(len(params), 1))()
-        for i, member in enumerate(params):
-            ps = (Param * max(len(member), 1))()
-            for j, (name, value) in enumerate(sorted(member.items())):
-                values = np.ascontiguousarray(np.atleast_1d(np.asarray(value, np.float32)))
-                b = name.encode()
-                keep += [b, values]
-                ps[j] = Param(b, values.size, values.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
-            keep.append(ps)
-            mps[i] = MemberParams(len(member), ps)
+        """params: per member {name: float or sequence}, or those already
+        marshalled once by PreparedParams; entries: {name: ndarray}."""
+        if not isinstance(params, PreparedParams):
+            params = PreparedParams(params)
+        mps, keep = params.members, [params]
         ts = (Tensor * max(len(entries), 1))()
         for i, (name, array) in enumerate(entries.items()):
             a = np.ascontiguousarray(array)
@@ -357,7 +371,7 @@ class Context:
         callback = DONE_FN(done) if done else DONE_FN()
         handle = ctypes.c_void_p()
         buf = _errbuf()
-        status = load().nxs_run_async(self._handle, segment, len(params), mps, len(entries), ts,
+        status = load().nxs_run_async(self._handle, segment, params.count, mps, len(entries), ts,
                                       callback, None, tag, ctypes.byref(handle), buf, 1024)
         _check(status, buf)
         return Request(handle, callback)

@@ -154,6 +154,7 @@ class CudaSegment:
         self.specs = specs
         self.geometry = geometry
         self.inputs = _inputs(members_, geometry)
+        self._prepared = None  # (inputs, their PreparedParams)
         self.times_us = []
         self._finalizer = weakref.finalize(self, _release, device, self.id)
 
@@ -220,8 +221,13 @@ class CudaSegment:
             except native.NativeError as error:
                 return ("ok", _Refused(error.message))
             segment.configured_version = segment.version
+        # The params are marshalled again only when they change (reload and
+        # put_member_state give the segment a new inputs list).
+        prepared = segment._prepared
+        if prepared is None or prepared[0] is not segment.inputs:
+            prepared = segment._prepared = (segment.inputs, native.PreparedParams(segment.inputs))
         try:
-            request = ctx.run_async(segment.id, segment.inputs, dict(tensors))
+            request = ctx.run_async(segment.id, prepared[1], dict(tensors))
         except native.NativeError as error:
             return ("ok", _Failed(error.message))
         return ("ok", request)

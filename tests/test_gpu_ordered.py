@@ -63,6 +63,22 @@ def test_ordered_costs(native, oracle, span, disparities):
     assert (g.host(d_costs) == permuted(want, span)).all()
 
 
+@pytest.mark.parametrize("span", [0, 8, 16])
+@pytest.mark.parametrize("disparities", [16, 64, 96, 128, 192, 256])
+@pytest.mark.parametrize("w,h", [(70, 23), (9, 7), (131, 5), (300, 17)])
+def test_census_and_costs_in_one_launch(native, oracle, span, disparities, w, h):
+    """nxs_census_costs_device_ordered forms the codes in shared memory: its
+    costs equal the oracle's census then costs, at widths below, across and
+    not a multiple of its 128-pixel blocks and of the census's four pixels."""
+    left, right = oracle.scene(w, h, 11)
+    d_left, d_right = g.dev(left), g.dev(right)
+    d_costs = g.empty((h, w, disparities), g.torch().uint8)
+    native.call("nxs_census_costs_device_ordered", g.ptr(d_left), g.ptr(d_right), w, h,
+                disparities, span, g.ptr(d_costs), g.stream())
+    want = oracle.costs(oracle.census(left), oracle.census(right), disparities).astype(np.uint8)
+    assert (g.host(d_costs) == permuted(want, span)).all()
+
+
 @pytest.mark.parametrize("span", [8, 16])
 @pytest.mark.parametrize("disparities,paths", [(64, 8), (128, 8), (128, 3), (256, 8), (96, 8)])
 def test_ordered_paths_and_selection(native, oracle, span, disparities, paths):
@@ -98,3 +114,7 @@ def test_the_matchers_span(native):
         assert lib.nxs_matcher_span(d) == (8 if lib.nxs_path_words(d) == 4 else 16)
     with pytest.raises(native.NativeError):
         native.call("nxs_costs_device_ordered", 1, 1, 8, 8, 64, 4, 1, None)
+    with pytest.raises(native.NativeError):  # a span the kernels do not take
+        native.call("nxs_census_costs_device_ordered", 1, 1, 8, 8, 64, 4, 1, None)
+    with pytest.raises(native.NativeError):  # not a multiple of 16 disparities
+        native.call("nxs_census_costs_device_ordered", 1, 1, 8, 8, 72, 16, 1, None)
