@@ -274,6 +274,9 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         stage_ms = {name: statistics.mean(m[k].elapsed_time(m[k + 1]) for m in stage_marks)
                     for k, name in enumerate(DevicePipeline.STAGES)}
+    # The clock record covers the device-timed steps; the sampler's reader
+    # thread stops before the host-bound end-to-end loop.
+    sampler.stop()
     total_s = replicas.max_over_ranks(sum(step_ms) / 1000.0, device="cuda")
     value = replicas.whole_job_rate(args.steps, world, total_s)
 
@@ -323,7 +326,6 @@ def run_ours(args, rank, world, local_rank):
         if collecting:
             gc.enable()
     e_s = replicas.max_over_ranks(e_elapsed, device="cuda")
-    sampler.stop()
     clocks = sampler.summary(t0, t1)
     seg.release()
 

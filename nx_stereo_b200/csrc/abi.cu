@@ -7,10 +7,12 @@
 // temporal filter's previous disparity and missed counts, the quality
 // stage's previous disparity). A request copies its entries into pinned
 // memory, enqueues the upload into its slot, every member's kernels and the
-// download of the outputs, ordered by events, and returns. Compute runs on
-// one stream in request order, as the reference's Port computes them
-// (native/stereo_match/src/main.rs:1-11), while uploads and downloads of
-// neighbouring requests overlap it.
+// download of the outputs, ordered by events, and returns. A segment whose
+// stages carry state computes on one stream in request order, as the
+// reference's Port computes them (native/stereo_match/src/main.rs:1-11); one
+// whose stages carry nothing alternates its requests between two compute
+// streams. Uploads and downloads of neighbouring requests overlap the compute,
+// and replies complete in request order.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -174,16 +176,24 @@ struct Slot {
     float *disparity[2] = {nullptr, nullptr}, *grid = nullptr, *quality_sums = nullptr;
     uint16_t *depth_mm = nullptr;
     int32_t *kept = nullptr;
+    // The entries, and the outputs, each in one region (Segment::entry_at and
+    // output_at): the buffers above that are entries or outputs lie inside them.
+    uint8_t *entries = nullptr, *outputs = nullptr;
     cudaEvent_t entered = nullptr;   // entries on the device
-    cudaEvent_t computed = nullptr;  // outputs ready
     cudaEvent_t free = nullptr;      // outputs downloaded: the slot may be reused
 };
 
 // Requests cycle through kSlots slots. Entries go up on `upload`, the members
-// compute on `stream`, outputs come down on `download`: request n + 1's
-// upload and compute overlap request n's download. Compute is in request
-// order on one stream, so what the stages carry advances pair by pair.
+// compute on a compute stream, outputs come down on `download`: request n + 1's
+// upload and compute overlap request n's download. A segment whose stages
+// carry state from pair to pair (TemporalFilter, Quality) computes on one
+// stream in request order, so that state advances pair by pair; one whose
+// stages carry nothing computes request n on stream n mod kLanes, each with
+// its own matcher scratch and depth map, so neighbouring pairs overlap on the
+// device (each pair's result is the same as alone). Downloads stay in request
+// order on one stream.
 constexpr int kSlots = 4;
+constexpr int kLanes = 2;
 
 struct Segment {
     uint32_t id = 0;
@@ -191,16 +201,32 @@ struct Segment {
     nxs_geometry g{};
     std::vector<Member> members;
     std::vector<Spec> entries, outputs;
-    cudaStream_t stream = nullptr, upload = nullptr, download = nullptr;
+    cudaStream_t upload = nullptr, download = nullptr;
+    cudaStream_t lanes[kLanes] = {};  // compute streams, n_lanes of them
+    int n_lanes = 1;
     std::mutex order;  // one request enqueued at a time
     uint64_t sequence = 0;
     PinnedPool pinned;
     EventPool events;
     Slot slots[kSlots];
-    // shared by every request, touched only on `stream`
-    float *depth_m = nullptr, *quality_columns = nullptr;
-    DeviceBuffer scratch;
+    // A request's entries go up in one copy and its outputs come down in one:
+    // each has a region per slot and a pinned block per request, laid out
+    // alike (offsets 256-byte aligned, in the order of `entries` and `outputs`).
+    // The outputs are one region unless one of them is also an entry (a
+    // disparity passed in and out unfiltered); then each comes down on its own.
+    std::vector<size_t> entry_at, output_at;
+    size_t entry_bytes = 0, output_bytes = 0;
+    bool outputs_packed = false;
+    // shared by the requests of one compute lane, touched only on its stream
+    float *depth_m[kLanes] = {}, *quality_columns = nullptr;
+    DeviceBuffer scratch[kLanes];
     std::vector<void *> allocations;
+
+    std::vector<cudaStream_t> streams() const {
+        std::vector<cudaStream_t> all = {upload, download};
+        for (int k = 0; k < n_lanes; ++k) all.push_back(lanes[k]);
+        return all;
+    }
 
     template <typename T>
     cudaError_t alloc(T **p, size_t count) {
@@ -214,14 +240,14 @@ struct Segment {
     }
     ~Segment() {
         cudaSetDevice(device);
-        for (cudaStream_t st : {upload, stream, download})
+        for (cudaStream_t st : streams())
             if (st) cudaStreamSynchronize(st);
         for (void *p : allocations) cudaFree(p);
-        scratch.release();
+        for (DeviceBuffer &b : scratch) b.release();
         for (Slot &slot : slots)
-            for (cudaEvent_t ev : {slot.entered, slot.computed, slot.free})
+            for (cudaEvent_t ev : {slot.entered, slot.free})
                 if (ev) cudaEventDestroy(ev);
-        for (cudaStream_t st : {upload, stream, download})
+        for (cudaStream_t st : streams())
             if (st) cudaStreamDestroy(st);
     }
 };
@@ -1032,8 +1058,14 @@ extern "C" nxs_status nxs_configure(nxs_context *c, uint32_t id, const nxs_geome
     }
     cudaSetDevice(c->device);
     cudaError_t e = cudaSuccess;
-    for (cudaStream_t *st : {&seg->upload, &seg->stream, &seg->download})
+    bool carries = false;
+    for (const Member &m : seg->members)
+        carries = carries || m.kind == Kind::Temporal || m.kind == Kind::Quality;
+    seg->n_lanes = carries ? 1 : kLanes;
+    for (cudaStream_t *st : {&seg->upload, &seg->download})
         if (!e) e = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
+    for (int k = 0; k < seg->n_lanes; ++k)
+        if (!e) e = cudaStreamCreateWithFlags(&seg->lanes[k], cudaStreamNonBlocking);
     const size_t pixels = (size_t)g.width * g.height;
     const size_t frame = (size_t)g.frame_width * g.frame_height;
     int max_disparities = 0, decimation = 1;
@@ -1041,24 +1073,83 @@ extern "C" nxs_status nxs_configure(nxs_context *c, uint32_t id, const nxs_geome
         if (m.kind == Kind::Disparity) max_disparities = std::max(max_disparities, m.disparities);
         if (m.kind == Kind::Cloud) decimation = m.decimation;
     }
+    // Each speckle filter moves the disparity to the slot's other buffer.
+    int final_disparity = 0;
+    for (const Member &m : seg->members)
+        if (m.kind == Kind::Speckle) final_disparity = 1 - final_disparity;
+    // Bytes of each named buffer (the point cloud's grid with one spare point).
+    const size_t grid_bytes = 4 * 3 * (pixels / (decimation * decimation) + 1);
+    auto buffer_bytes = [&](const std::string &name) -> size_t {
+        if (name == "left_frame" || name == "right_frame") return std::max<size_t>(frame, 1);
+        if (name == "left" || name == "right") return pixels;
+        if (name == "disparity") return 4 * pixels;
+        if (name == "depth_mm") return 2 * pixels;
+        if (name == "cloud_grid") return grid_bytes;
+        if (name == "cloud_points") return 4;
+        return 4 * 5;  // quality_sums
+    };
+    auto round256 = [](size_t n) { return (n + 255) & ~(size_t)255; };
+    seg->entry_bytes = seg->output_bytes = 0;
+    for (const Spec &spec : seg->entries) {
+        seg->entry_at.push_back(seg->entry_bytes);
+        seg->entry_bytes += round256(buffer_bytes(spec.name));
+    }
+    seg->outputs_packed = true;
+    for (const Spec &spec : seg->outputs) {
+        seg->output_at.push_back(seg->output_bytes);
+        seg->output_bytes += round256(buffer_bytes(spec.name));
+        for (const Spec &entry : seg->entries)  // a buffer both an entry and an output
+            if (entry.name == spec.name && (spec.name != "disparity" || final_disparity == 0))
+                seg->outputs_packed = false;
+    }
     for (Slot &slot : seg->slots) {
-        if (!e) e = seg->alloc(&slot.frames[0], std::max<size_t>(frame, 1));
-        if (!e) e = seg->alloc(&slot.frames[1], std::max<size_t>(frame, 1));
-        if (!e) e = seg->alloc(&slot.images[0], pixels);
-        if (!e) e = seg->alloc(&slot.images[1], pixels);
-        if (!e) e = seg->alloc(&slot.disparity[0], pixels);
-        if (!e) e = seg->alloc(&slot.disparity[1], pixels);
-        if (!e) e = seg->alloc(&slot.depth_mm, pixels);
-        if (!e) e = seg->alloc(&slot.grid, 3 * (pixels / (decimation * decimation) + 1));
-        if (!e) e = seg->alloc(&slot.kept, 1);
-        if (!e) e = seg->alloc(&slot.quality_sums, 5);
-        for (cudaEvent_t *ev : {&slot.entered, &slot.computed, &slot.free})
+        if (!e && seg->entry_bytes) e = seg->alloc(&slot.entries, seg->entry_bytes);
+        if (!e && seg->outputs_packed && seg->output_bytes)
+            e = seg->alloc(&slot.outputs, seg->output_bytes);
+        // A named buffer lies in the entry region when it is an entry, else in the
+        // output region when it is an output, else on its own.
+        auto place = [&](const char *entry, const char *output, const std::string &name,
+                         void **at) -> cudaError_t {
+            for (size_t k = 0; entry && k < seg->entries.size(); ++k)
+                if (seg->entries[k].name == entry) {
+                    *at = slot.entries + seg->entry_at[k];
+                    return cudaSuccess;
+                }
+            for (size_t k = 0; output && seg->outputs_packed && k < seg->outputs.size(); ++k)
+                if (seg->outputs[k].name == output) {
+                    *at = slot.outputs + seg->output_at[k];
+                    return cudaSuccess;
+                }
+            uint8_t *own = nullptr;
+            cudaError_t err = seg->alloc(&own, buffer_bytes(name));
+            *at = own;
+            return err;
+        };
+        const char *disparity_out[2] = {final_disparity == 0 ? "disparity" : nullptr,
+                                        final_disparity == 1 ? "disparity" : nullptr};
+        struct Named { const char *entry, *output, *name; void **at; } named[] = {
+            {"left_frame", nullptr, "left_frame", (void **)&slot.frames[0]},
+            {"right_frame", nullptr, "right_frame", (void **)&slot.frames[1]},
+            {"left", "left", "left", (void **)&slot.images[0]},
+            {"right", "right", "right", (void **)&slot.images[1]},
+            {"disparity", disparity_out[0], "disparity", (void **)&slot.disparity[0]},
+            {nullptr, disparity_out[1], "disparity", (void **)&slot.disparity[1]},
+            {nullptr, "depth_mm", "depth_mm", (void **)&slot.depth_mm},
+            {nullptr, "cloud_grid", "cloud_grid", (void **)&slot.grid},
+            {nullptr, "cloud_points", "cloud_points", (void **)&slot.kept},
+            {nullptr, "quality_sums", "quality_sums", (void **)&slot.quality_sums},
+        };
+        for (const Named &b : named)
+            if (!e) e = place(b.entry, b.output, b.name, b.at);
+        for (cudaEvent_t *ev : {&slot.entered, &slot.free})
             if (!e) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
     }
-    if (!e) e = seg->alloc(&seg->depth_m, pixels);
+    for (int k = 0; k < seg->n_lanes; ++k) {
+        if (!e) e = seg->alloc(&seg->depth_m[k], pixels);
+        if (!e && max_disparities)
+            e = seg->scratch[k].reserve(matcher_scratch_bytes(g.width, g.height, max_disparities));
+    }
     if (!e) e = seg->alloc(&seg->quality_columns, 5 * (size_t)g.width);
-    if (!e && max_disparities)
-        e = seg->scratch.reserve(matcher_scratch_bytes(g.width, g.height, max_disparities));
     // What the stages carry starts over: previous = -1, missed = 0
     // (stage/temporal_filter.ex:219-226, stage/quality.ex:144-145).
     for (Member &m : seg->members) {
@@ -1078,8 +1169,11 @@ extern "C" nxs_status nxs_configure(nxs_context *c, uint32_t id, const nxs_geome
     if (!e) {  // pinned staging for 2 x kSlots requests: those in flight and those read out
         std::vector<size_t> blocks;
         for (int k = 0; k < 2 * kSlots; ++k) {
-            for (const Spec &spec : seg->entries) blocks.push_back(spec.bytes());
-            for (const Spec &spec : seg->outputs) blocks.push_back(std::max<size_t>(spec.bytes(), 4));
+            blocks.push_back(std::max<size_t>(seg->entry_bytes, 4));
+            if (seg->outputs_packed) blocks.push_back(std::max<size_t>(seg->output_bytes, 4));
+            else
+                for (const Spec &spec : seg->outputs)
+                    blocks.push_back(std::max<size_t>(spec.bytes(), 4));
         }
         e = seg->pinned.reserve(blocks);
     }
@@ -1171,17 +1265,27 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
     if (!e) e = seg->events.take(false, &r->done);
     // Stage the entries in pinned memory now: the caller's buffers are only
     // borrowed for the call.
-    std::vector<void *> staged(seg->entries.size(), nullptr);
-    for (size_t k = 0; k < seg->entries.size() && !e; ++k) {
-        staged[k] = seg->pinned.take(seg->entries[k].bytes());
-        if (!staged[k]) e = cudaErrorMemoryAllocation;
+    uint8_t *staged = nullptr;
+    if (!e) {
+        staged = static_cast<uint8_t *>(seg->pinned.take(std::max<size_t>(seg->entry_bytes, 4)));
+        if (!staged) e = cudaErrorMemoryAllocation;
+        else r->pinned.push_back(staged);
+    }
+    for (size_t k = 0; k < seg->entries.size() && !e; ++k)
+        memcpy(staged + seg->entry_at[k], matched[k]->data, seg->entries[k].bytes());
+    std::vector<void *> out_host(seg->outputs.size(), nullptr);
+    uint8_t *out_block = nullptr;  // the outputs' one pinned block, when packed
+    if (!e && seg->outputs_packed) {
+        out_block =
+            static_cast<uint8_t *>(seg->pinned.take(std::max<size_t>(seg->output_bytes, 4)));
+        if (!out_block) e = cudaErrorMemoryAllocation;
         else {
-            memcpy(staged[k], matched[k]->data, seg->entries[k].bytes());
-            r->pinned.push_back(staged[k]);
+            r->pinned.push_back(out_block);
+            for (size_t k = 0; k < seg->outputs.size(); ++k)
+                out_host[k] = out_block + seg->output_at[k];
         }
     }
-    std::vector<void *> out_host(seg->outputs.size(), nullptr);
-    for (size_t k = 0; k < seg->outputs.size() && !e; ++k) {
+    for (size_t k = 0; k < seg->outputs.size() && !e && !seg->outputs_packed; ++k) {
         out_host[k] = seg->pinned.take(std::max<size_t>(seg->outputs[k].bytes(), 4));
         if (!out_host[k]) e = cudaErrorMemoryAllocation;
         else r->pinned.push_back(out_host[k]);
@@ -1192,23 +1296,18 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
     }
 
     std::lock_guard<std::mutex> order(seg->order);
-    Slot &slot = seg->slots[seg->sequence++ % kSlots];
-    cudaStream_t s = seg->stream;
+    const uint64_t sequence = seg->sequence++;
+    Slot &slot = seg->slots[sequence % kSlots];
+    const int lane = (int)(sequence % (uint64_t)seg->n_lanes);
+    cudaStream_t s = seg->lanes[lane];
     const size_t pixels = (size_t)g.width * g.height;
     // Upload, once the slot's last request has downloaded its outputs.
     e = cudaStreamWaitEvent(seg->upload, slot.free, 0);
-    for (size_t k = 0; k < seg->entries.size() && !e; ++k) {
-        const std::string &name = seg->entries[k].name;
-        void *dst = name == "left_frame" ? (void *)slot.frames[0]
-                    : name == "right_frame" ? (void *)slot.frames[1]
-                    : name == "left"        ? (void *)slot.images[0]
-                    : name == "right"       ? (void *)slot.images[1]
-                                            : (void *)slot.disparity[0];
-        e = cudaMemcpyAsync(dst, staged[k], seg->entries[k].bytes(), cudaMemcpyHostToDevice,
+    if (!e && seg->entry_bytes)
+        e = cudaMemcpyAsync(slot.entries, staged, seg->entry_bytes, cudaMemcpyHostToDevice,
                             seg->upload);
-    }
     if (!e) e = cudaEventRecord(slot.entered, seg->upload);
-    // Compute, in request order.
+    // Compute on the request's lane.
     if (!e) e = cudaStreamWaitEvent(s, slot.entered, 0);
     int current = 0;  // which of the slot's disparity buffers holds the disparity so far
     for (size_t i = 0; i < n && !e; ++i) {
@@ -1224,7 +1323,7 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
             break;
         case Kind::Disparity: {
             MatcherScratch ms =
-                carve_matcher_scratch(seg->scratch.ptr, g.width, g.height, m.disparities);
+                carve_matcher_scratch(seg->scratch[lane].ptr, g.width, g.height, m.disparities);
             e = run_matcher(slot.images[0], slot.images[1], g.width, g.height, m.disparities,
                             m.paths, l.sgm.p1, l.sgm.p2, l.sgm.uniqueness, 1, ms,
                             slot.disparity[current], s);
@@ -1241,10 +1340,10 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
             break;
         case Kind::Depth:
             e = launch_depth(slot.disparity[current], pixels, l.a, l.b, slot.depth_mm,
-                             seg->depth_m, s);
+                             seg->depth_m[lane], s);
             break;
         case Kind::Cloud:
-            e = launch_cloud(seg->depth_m, g.width, g.height, m.decimation, l.a, l.b, l.c,
+            e = launch_cloud(seg->depth_m[lane], g.width, g.height, m.decimation, l.a, l.b, l.c,
                              m.min_depth_m, m.max_depth_m, slot.grid, slot.kept, s);
             break;
         case Kind::Quality:
@@ -1253,10 +1352,12 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
             break;
         }
     }
-    if (!e) e = cudaEventRecord(r->marks[n], s);
-    if (!e) e = cudaEventRecord(slot.computed, s);
-    // Download the outputs into the request's pinned blocks.
-    if (!e) e = cudaStreamWaitEvent(seg->download, slot.computed, 0);
+    if (!e) e = cudaEventRecord(r->marks[n], s);  // the last member done: outputs ready
+    // Download the outputs into the request's pinned block(s).
+    if (!e) e = cudaStreamWaitEvent(seg->download, r->marks[n], 0);
+    if (!e && seg->outputs_packed && seg->output_bytes)
+        e = cudaMemcpyAsync(out_block, slot.outputs, seg->output_bytes, cudaMemcpyDeviceToHost,
+                            seg->download);
     r->outputs.resize(seg->outputs.size());
     r->names.resize(seg->outputs.size());
     for (size_t k = 0; k < seg->outputs.size() && !e; ++k) {
@@ -1268,8 +1369,9 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
                           : spec.name == "cloud_grid"   ? (const void *)slot.grid
                           : spec.name == "cloud_points" ? (const void *)slot.kept
                                                         : (const void *)slot.quality_sums;
-        e = cudaMemcpyAsync(out_host[k], src, spec.bytes(), cudaMemcpyDeviceToHost,
-                            seg->download);
+        if (!seg->outputs_packed)
+            e = cudaMemcpyAsync(out_host[k], src, spec.bytes(), cudaMemcpyDeviceToHost,
+                                seg->download);
         r->names[k] = spec.name;
         nxs_tensor &t = r->outputs[k];
         t.name = r->names[k].c_str();
@@ -1285,7 +1387,7 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
     if (!e && done) e = cudaLaunchHostFunc(seg->download, request_done, r);
     if (e) {
         // The streams are still ordered: wait for what was enqueued before freeing.
-        for (cudaStream_t st : {seg->upload, seg->stream, seg->download}) cudaStreamSynchronize(st);
+        for (cudaStream_t st : seg->streams()) cudaStreamSynchronize(st);
         nxs_request_free(r);
         return cuda_status(e, error, error_len, "enqueueing the request");
     }
@@ -1384,6 +1486,6 @@ extern "C" nxs_status nxs_release(nxs_context *c, uint32_t id) {
         c->segments.erase(it);
     }
     cudaSetDevice(c->device);
-    for (cudaStream_t st : {seg->upload, seg->stream, seg->download}) cudaStreamSynchronize(st);
+    for (cudaStream_t st : seg->streams()) cudaStreamSynchronize(st);
     return NXS_OK;
 }

@@ -6,7 +6,10 @@ A pair goes through a segment in three steps, as in the reference:
 `send_request` hands its entries to the device without waiting,
 `await_`/`response` recognise its reply, and `collect` returns what it
 brought back; `run` does all three. Up to `depth()` pairs may be at the
-device at once, computed in the order sent. A reply ("error", reason) fails
+device at once, and their replies complete in the order sent: a segment
+whose stages carry state from pair to pair computes them one after another,
+one whose stages carry nothing computes neighbouring pairs at once on two
+streams. A reply ("error", reason) fails
 that pair only; ("stop", reason) says the device refuses the segment itself.
 """
 import itertools

@@ -164,6 +164,10 @@ def test_pairs_in_flight_equal_pairs_sent_alone(seg_mod, oracle):
         reply = seg_mod.CudaSegment.await_(request, segment_, 60000)
         assert reply[0] == "ok", reply
         together.append({k: np.array(v) for k, v in reply[1].items()})
+    # These stages carry nothing, so neighbouring pairs compute on two streams at
+    # once; their replies still complete in the order sent.
+    stamps = [request.done_ns() for request in sent]
+    assert all(stamps) and stamps == sorted(stamps)
     for (left, right), got in zip(pairs, together):
         _, alone_segment = seg_mod.CudaSegment.build(members, geometry)
         alone, _ = run(seg_mod, alone_segment, {"left": left, "right": right})
