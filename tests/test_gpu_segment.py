@@ -95,6 +95,48 @@ def test_stateful_pipeline_keeps_history_through_updates_and_reload(seg_mod):
     segment_.release()
 
 
+def test_disparity_entries_in_either_output_layout(seg_mod, oracle):
+    """A disparity passed in: TemporalFilter -> Depth also returns it (the entry's
+    buffer is an output, so each output comes down on its own); Depth ->
+    PointCloud does not (one packed download, and the pairs, sent together,
+    compute on two streams). Each against the oracle, pair by pair."""
+    from nx_stereo_b200 import stage
+
+    w, h = 40, 24
+    geometry = dict(GEOMETRY, width=w, height=h, frame_width=w, frame_height=h,
+                    principal_point=(19.5, 11.5))
+    rng = np.random.default_rng(5)
+    maps = [np.where(rng.random((h, w)) < 0.2, -1.0, rng.uniform(1.0, 60.0, (h, w)))
+            .astype(np.float32) for _ in range(5)]
+    _, members = seg_mod.members([stage.TemporalFilter, stage.Depth], geometry)
+    _, temporal_segment = seg_mod.CudaSegment.build(members, geometry)
+    previous, missed = np.full((h, w), -1.0, np.float32), np.zeros((h, w), np.float32)
+    for current in maps:
+        output, temporal_segment = run(seg_mod, temporal_segment, {"disparity": current})
+        want, previous, missed = oracle.temporal(current, previous, missed)
+        assert g.same_bits(output["disparity"], want)
+        assert (output["depth_mm"] == oracle.depth(want, 64.0, 0.125)[0]).all()
+    temporal_segment.release()
+
+    _, members = seg_mod.members([stage.Depth, (stage.PointCloud, {"decimation": 2})], geometry)
+    _, cloud_segment = seg_mod.CudaSegment.build(members, geometry)
+    sent = []
+    for current in maps:
+        status, request = seg_mod.CudaSegment.send_request({"disparity": current}, cloud_segment)
+        assert status == "ok"
+        sent.append(request)
+    for current, request in zip(maps, sent):
+        reply = seg_mod.CudaSegment.await_(request, cloud_segment, 60000)
+        assert reply[0] == "ok", reply
+        depth_mm, depth_m = oracle.depth(current, 64.0, 0.125)
+        grid, kept = oracle.cloud(depth_m, 2, 64.0, 19.5, 11.5)
+        assert (reply[1]["depth_mm"] == depth_mm).all()
+        assert int(reply[1]["cloud_points"]) == kept
+        got, empty = reply[1]["cloud_grid"], np.isnan(grid)
+        assert (np.isnan(got) == empty).all() and g.same_bits(got[~empty], grid[~empty])
+    cloud_segment.release()
+
+
 # ---------------------------------------------------------------- full pipelines vs the oracle
 def _oracle_chain(oracle, geometry, frames, disparities, paths, temporal=None, quality=None):
     h, w = geometry["height"], geometry["width"]
