@@ -180,22 +180,29 @@ __host__ __device__ constexpr int span_position(int span, int d) {
     return span == 0 ? d : (d / span) * span + 2 * ((d % span) % (span / 2)) + (d % span) / (span / 2);
 }
 
+// Where code j of a staged code array (lefts, rights below) lies: within each
+// 128-byte block of 8 code pairs, an odd block swaps neighbouring pairs, so that
+// the 16-byte pair reads of eight threads whose windows start 4 codes apart fall
+// in 8 different bank quads (checked on the CPU for 16..256 disparities).
+__host__ __device__ constexpr int code_slot(int j) { return j ^ ((j >> 3) & 2); }
+__host__ __device__ constexpr int pair_slot(int pair) { return pair ^ ((pair >> 3) & 1); }
+
 __host__ __device__ inline size_t costs_shared_bytes(int disparities) {
     return sizeof(uint64_t) * (2 * kCostPixels + disparities) + (size_t)kCostPixels * disparities;
 }
 
 // Costs of PIXELS pixels of row y from x0 on, from codes staged in shared
-// memory (16-byte aligned): lefts[i] the code of x0 + i (0 past the image),
-// rights[i] that of x0 - D + i (0 outside it), PIXELS + D of them; `tile`
-// (16-byte aligned) takes PIXELS x D bytes.
+// memory (16-byte aligned): lefts[code_slot(i)] the code of x0 + i (0 past the
+// image), rights[code_slot(i)] that of x0 - D + i (0 outside it), PIXELS + D of
+// them; `tile` (16-byte aligned) takes PIXELS x D bytes.
 //
-// Shared-memory banks: a warp's threads take 32 neighbouring groups of 4
-// pixels at one run of 16 disparities. Their code windows start 4 codes (32
-// bytes) apart and are read as 16-byte pairs, so a read serves 4 threads per
-// 128 bytes. Each tile row is D bytes with its 16-byte runs rotated by the
-// pixel's group (run q of pixel p at (q + p / 4) mod D / 16), so a warp's
-// 16-byte stores to four pixel rows fall in 8 different bank quads; the
-// write-out undoes the rotation.
+// Shared-memory banks: a warp's threads take neighbouring groups of 4 pixels at
+// one run of 16 disparities. Their code windows start 4 codes (32 bytes) apart
+// and are read as 16-byte pairs, which code_slot's layout spreads over all bank
+// quads. Each tile row is D bytes with its 16-byte runs rotated by the pixel's
+// group (run q of pixel p at (q + p / 4) mod D / 16), so a warp's 16-byte stores
+// to four pixel rows fall in 8 different bank quads; the write-out undoes the
+// rotation.
 template <int SPAN, int PIXELS>
 __device__ __forceinline__ void costs_from_codes(const uint64_t *lefts, const uint64_t *rights,
                                                  int width, int disparities,
@@ -211,16 +218,18 @@ __device__ __forceinline__ void costs_from_codes(const uint64_t *lefts, const ui
         // pixel p0 + i at disparity d0 + k reads rights[p0 + i - d0 - k + D]
         //   = window[16 + i - k], window[m] = rights[p0 - d0 + D - 16 + m]
         // (m = 1..19; the first of the 20 is read for the 16-byte alignment)
-        const uint4 *base = reinterpret_cast<const uint4 *>(rights + p0 - d0 + D - 16);
+        const uint4 *pairs = reinterpret_cast<const uint4 *>(rights);
+        const int first = (p0 - d0 + D - 16) / 2;  // the window's first pair
         uint64_t window[20];
 #pragma unroll
         for (int j = 0; j < 10; ++j) {
-            const uint4 two = base[j];
+            const uint4 two = pairs[pair_slot(first + j)];
             window[2 * j] = (uint64_t)two.x | (uint64_t)two.y << 32;
             window[2 * j + 1] = (uint64_t)two.z | (uint64_t)two.w << 32;
         }
-        const uint4 *left_pairs = reinterpret_cast<const uint4 *>(lefts + p0);
-        const uint4 l01 = left_pairs[0], l23 = left_pairs[1];
+        const uint4 *left_pairs = reinterpret_cast<const uint4 *>(lefts);
+        const uint4 l01 = left_pairs[pair_slot(2 * group)];
+        const uint4 l23 = left_pairs[pair_slot(2 * group + 1)];
         const uint64_t l4[4] = {(uint64_t)l01.x | (uint64_t)l01.y << 32,
                                 (uint64_t)l01.z | (uint64_t)l01.w << 32,
                                 (uint64_t)l23.x | (uint64_t)l23.y << 32,
@@ -266,10 +275,10 @@ __device__ __forceinline__ void costs_tile(const uint64_t *__restrict__ left_cod
     uint8_t *tile = staged + sizeof(uint64_t) * (2 * kCostPixels + D);
     const size_t row = (size_t)y * width;
     for (int i = threadIdx.x; i < kCostPixels; i += blockDim.x)
-        lefts[i] = x0 + i < width ? __ldcg(left_codes + row + x0 + i) : 0;
+        lefts[code_slot(i)] = x0 + i < width ? __ldcg(left_codes + row + x0 + i) : 0;
     for (int i = threadIdx.x; i < kCostPixels + D; i += blockDim.x) {
         const int x = x0 - D + i;
-        rights[i] = (x >= 0 && x < width) ? __ldcg(right_codes + row + x) : 0;
+        rights[code_slot(i)] = (x >= 0 && x < width) ? __ldcg(right_codes + row + x) : 0;
     }
     __syncthreads();
     costs_from_codes<SPAN, kCostPixels>(lefts, rights, width, D, costs, x0, y, tile);
@@ -322,14 +331,15 @@ __device__ __forceinline__ void census_costs_tile(const uint8_t *__restrict__ le
         if (g < kLeftGroups) {
             census4(left_window, left_pitch, 4 * g + 4, 3, four);
 #pragma unroll
-            for (int i = 0; i < 4; ++i) lefts[4 * g + i] = x0 + 4 * g + i < width ? four[i] : 0;
+            for (int i = 0; i < 4; ++i)
+                lefts[code_slot(4 * g + i)] = x0 + 4 * g + i < width ? four[i] : 0;
         } else {
             const int r = g - kLeftGroups;
             census4(right_window, right_pitch, 4 * r + 4, 3, four);
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const int x = x0 - D + 4 * r + i;
-                rights[4 * r + i] = (x >= 0 && x < width) ? four[i] : 0;
+                rights[code_slot(4 * r + i)] = (x >= 0 && x < width) ? four[i] : 0;
             }
         }
     }
