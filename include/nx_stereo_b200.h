@@ -158,7 +158,8 @@ nxs_status nxs_request_times(nxs_request *request, uint32_t *n_members,
                              const uint32_t **times_us);
 
 /* When the device finished the request, in nanoseconds of CLOCK_MONOTONIC
- * (the clock of a serving loop's arrival times); 0 while it is pending. */
+ * (the clock of a serving loop's arrival times), from the device's timestamp
+ * of the request's completion mapped onto that clock; 0 while it is pending. */
 uint64_t nxs_request_done_ns(nxs_request *request);
 
 /* Frees a request; waits for it first if it is still on the device. */

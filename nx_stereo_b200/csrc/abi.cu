@@ -2,8 +2,9 @@
 // (configure / run / release, the reference Port's three requests) and the
 // direct entry points.
 //
-// A segment owns three CUDA streams (upload, compute, download), a ring of
-// per-request device slots and what its stages carry from pair to pair (the
+// A segment owns its CUDA streams (upload, one or two compute streams,
+// download, and a notify stream for the completion stamps and callbacks), a
+// ring of per-request device slots and what its stages carry from pair to pair (the
 // temporal filter's previous disparity and missed counts, the quality
 // stage's previous disparity). A request copies its entries into pinned
 // memory, enqueues the upload into its slot, every member's kernels and the
@@ -147,6 +148,70 @@ struct EventPool {
     }
 };
 
+uint64_t monotonic_ns() {
+    return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+// Maps the device's event timestamps onto CLOCK_MONOTONIC (steady_clock), the
+// clock of a serving loop's arrival times, with no host function in the
+// request's path: a reference event is recorded on an otherwise idle stream
+// and the host spins until it completes, five times, keeping the sample seen
+// in the narrowest window (its time is that window's midpoint, within a few
+// microseconds). A request's completion time is then the reference's time plus
+// the device's elapsed time from the reference to the request's done event. The
+// reference is taken again once it is 200 ms old, which bounds the drift
+// between the two clocks.
+struct DeviceClock {
+    std::mutex lock;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ref = nullptr, probe = nullptr;
+    uint64_t ref_ns = 0;
+    cudaError_t open() {
+        cudaError_t e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+        if (!e) e = cudaEventCreate(&ref);
+        if (!e) e = cudaEventCreate(&probe);
+        if (!e) e = calibrate();
+        return e;
+    }
+    cudaError_t calibrate() {
+        uint64_t best = UINT64_MAX;
+        for (int k = 0; k < 5; ++k) {
+            const uint64_t t0 = monotonic_ns();
+            cudaError_t e = cudaEventRecord(probe, stream);
+            if (e) return e;
+            while ((e = cudaEventQuery(probe)) == cudaErrorNotReady)
+                if (monotonic_ns() - t0 > 1000000000ull) return cudaErrorNotReady;
+            if (e) return e;
+            const uint64_t t1 = monotonic_ns();
+            if (t1 - t0 < best) {
+                best = t1 - t0;
+                std::swap(ref, probe);
+                ref_ns = t0 + (t1 - t0) / 2;
+            }
+        }
+        return cudaSuccess;
+    }
+    // CLOCK_MONOTONIC nanoseconds of a completed event; 0 if it cannot be read.
+    uint64_t at(cudaEvent_t event) {
+        std::lock_guard<std::mutex> g(lock);
+        if (monotonic_ns() - ref_ns > 200000000ull && calibrate()) return 0;
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, ref, event) == cudaSuccess)
+            return (uint64_t)((int64_t)ref_ns + llround((double)ms * 1e6));
+        if (cudaEventElapsedTime(&ms, event, ref) == cudaSuccess)  // before the reference
+            return (uint64_t)((int64_t)ref_ns - llround((double)ms * 1e6));
+        return 0;
+    }
+    ~DeviceClock() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (cudaEvent_t ev : {ref, probe})
+            if (ev) cudaEventDestroy(ev);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
 enum class Kind { Rectification, Disparity, Speckle, Temporal, Depth, Cloud, Quality };
 
 struct Member {
@@ -202,6 +267,11 @@ struct Segment {
     std::vector<Member> members;
     std::vector<Spec> entries, outputs;
     cudaStream_t upload = nullptr, download = nullptr;
+    // Runs the caller's completion callbacks (host functions), when a request
+    // has one, after its download, so that a host function waiting for the
+    // driver's callback thread holds up no later request's download.
+    cudaStream_t notify = nullptr;
+    DeviceClock clock;  // requests' completion times
     cudaStream_t lanes[kLanes] = {};  // compute streams, n_lanes of them
     int n_lanes = 1;
     std::mutex order;  // one request enqueued at a time
@@ -223,7 +293,7 @@ struct Segment {
     std::vector<void *> allocations;
 
     std::vector<cudaStream_t> streams() const {
-        std::vector<cudaStream_t> all = {upload, download};
+        std::vector<cudaStream_t> all = {upload, download, notify};
         for (int k = 0; k < n_lanes; ++k) all.push_back(lanes[k]);
         return all;
     }
@@ -276,7 +346,7 @@ struct nxs_request {
     nxs_done_fn callback = nullptr;
     void *user = nullptr;
     uint64_t tag = 0;
-    std::atomic<uint64_t> done_ns{0};  // CLOCK_MONOTONIC when the device finished it
+    std::atomic<uint64_t> done_ns{0};  // CLOCK_MONOTONIC of `done`, once read
 };
 
 // ---------------------------------------------------------------------------
@@ -1062,10 +1132,11 @@ extern "C" nxs_status nxs_configure(nxs_context *c, uint32_t id, const nxs_geome
     for (const Member &m : seg->members)
         carries = carries || m.kind == Kind::Temporal || m.kind == Kind::Quality;
     seg->n_lanes = carries ? 1 : kLanes;
-    for (cudaStream_t *st : {&seg->upload, &seg->download})
+    for (cudaStream_t *st : {&seg->upload, &seg->download, &seg->notify})
         if (!e) e = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
     for (int k = 0; k < seg->n_lanes; ++k)
         if (!e) e = cudaStreamCreateWithFlags(&seg->lanes[k], cudaStreamNonBlocking);
+    if (!e) e = seg->clock.open();
     const size_t pixels = (size_t)g.width * g.height;
     const size_t frame = (size_t)g.frame_width * g.frame_height;
     int max_disparities = 0, decimation = 1;
@@ -1188,15 +1259,6 @@ static void CUDART_CB request_done(void *data) {
     if (r->callback) r->callback(r->user, r->tag);
 }
 
-// Runs on the download stream before the request's done event is recorded,
-// so the event completes only after the stamp is written.
-static void CUDART_CB request_stamp(void *data) {
-    nxs_request *r = static_cast<nxs_request *>(data);
-    r->done_ns.store((uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
-                         std::chrono::steady_clock::now().time_since_epoch())
-                         .count());
-}
-
 extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_members,
                                     const nxs_member_params *params, uint32_t n_entries,
                                     const nxs_tensor *entries, nxs_done_fn done, void *user,
@@ -1262,7 +1324,7 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
     const size_t n = seg->members.size();
     r->marks.resize(n + 1, nullptr);
     for (size_t i = 0; i <= n && !e; ++i) e = seg->events.take(true, &r->marks[i]);
-    if (!e) e = seg->events.take(false, &r->done);
+    if (!e) e = seg->events.take(true, &r->done);  // timed: the completion time is read from it
     // Stage the entries in pinned memory now: the caller's buffers are only
     // borrowed for the call.
     uint8_t *staged = nullptr;
@@ -1382,9 +1444,9 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
         t.bytes = spec.bytes();
     }
     if (!e) e = cudaEventRecord(slot.free, seg->download);
-    if (!e) e = cudaLaunchHostFunc(seg->download, request_stamp, r);
     if (!e) e = cudaEventRecord(r->done, seg->download);
-    if (!e && done) e = cudaLaunchHostFunc(seg->download, request_done, r);
+    if (!e && done) e = cudaStreamWaitEvent(seg->notify, r->done, 0);
+    if (!e && done) e = cudaLaunchHostFunc(seg->notify, request_done, r);
     if (e) {
         // The streams are still ordered: wait for what was enqueued before freeing.
         for (cudaStream_t st : seg->streams()) cudaStreamSynchronize(st);
@@ -1452,7 +1514,16 @@ extern "C" nxs_status nxs_request_times(nxs_request *r, uint32_t *n_members,
     return NXS_OK;
 }
 
-extern "C" uint64_t nxs_request_done_ns(nxs_request *r) { return r ? r->done_ns.load() : 0; }
+extern "C" uint64_t nxs_request_done_ns(nxs_request *r) {
+    if (!r) return 0;
+    uint64_t ns = r->done_ns.load();
+    if (ns) return ns;
+    cudaSetDevice(r->segment->device);
+    if (cudaEventQuery(r->done) != cudaSuccess) return 0;
+    ns = r->segment->clock.at(r->done);
+    r->done_ns.store(ns);
+    return ns;
+}
 
 extern "C" nxs_status nxs_device_memory(nxs_context *c, uint64_t *free_bytes,
                                         uint64_t *total_bytes) {
@@ -1470,7 +1541,7 @@ extern "C" void nxs_request_free(nxs_request *r) {
     cudaSetDevice(r->segment->device);
     if (r->done) cudaEventSynchronize(r->done);
     for (cudaEvent_t ev : r->marks) r->segment->events.give(true, ev);
-    r->segment->events.give(false, r->done);
+    r->segment->events.give(true, r->done);
     for (void *p : r->pinned) r->segment->pinned.give(p);
     delete r;
 }

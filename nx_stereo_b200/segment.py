@@ -158,7 +158,8 @@ class CudaSegment:
         self.geometry = geometry
         self.inputs = _inputs(members_, geometry)
         self._prepared = None  # (inputs, their PreparedParams)
-        self.times_us = []
+        self._times = []
+        self._timed = None  # the last reply's request, until its member times are read
         self._finalizer = weakref.finalize(self, _release, device, self.id)
 
     # -- the behaviour's callbacks, as functions of the class (module-like)
@@ -253,7 +254,9 @@ class CudaSegment:
                 return "timeout"
             # Views of the request's pinned memory: the request lives as long as they do.
             outputs = request.outputs(copy=False)
-            segment.times_us = request.times_us()
+            # The member times are read from the device's events only when asked
+            # for (member_times): reading them costs host time on every pair.
+            segment._timed = request
         except native.NativeError as error:
             request.free()
             return ("error", error.message)
@@ -265,6 +268,13 @@ class CudaSegment:
     def collect(outputs, segment, timeout):
         """The reply brought the outputs back: nothing to download."""
         return ("ok", outputs)
+
+    @property
+    def times_us(self):
+        """Each member's device time (us) for the last pair replied to."""
+        if self._timed is not None:
+            self._times, self._timed = self._timed.times_us(), None
+        return self._times
 
     @staticmethod
     def member_times(segment):
