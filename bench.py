@@ -474,7 +474,8 @@ def bench_large(torch, ctx):
     pairs = [scene.rectified_pair(1920, 1080, seed=900 + i, rectangles=12, min_disparity=8,
                                   max_disparity=240, sigma=3.0) for i in range(8)]
     out = _plain_and_batched(torch, ctx, shapes, pairs, repeats=3,
-                             tuner_search={"order": (0, 1), "group_pairs": (1, 2)})
+                             tuner_search={"engine": (0, 1), "order": (0, 1),
+                                           "group_pairs": (1, 2)})
     out["workload"] = "8 pairs 1920x1080, 256 disparities, 8 paths"
     return out
 
