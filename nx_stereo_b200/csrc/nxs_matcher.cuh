@@ -520,13 +520,18 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
     };
 #pragma unroll
     for (int i = 0; i < kPrefetch - 1; ++i) fetch(i, active && i < length);
-    for (int base = 0; base < steps; base += kPrefetch) {
+    // One block of kPrefetch steps from `base`. CHECKED: the steps test the warp's
+    // last step and each line's end; without, every line of the warp covers the
+    // block and the copies it starts (FULL: every lane active).
+    auto block = [&](const int base, auto checked) {
+        constexpr bool CHECKED = decltype(checked)::value;
 #pragma unroll
         for (int i = 0; i < kPrefetch; ++i) {
             const int step = base + i;
-            if (step >= steps) break;  // uniform across the warp
+            if (CHECKED && step >= steps) break;  // uniform across the warp
             // the copy of step + kPrefetch - 1 goes to the slot read last step
-            fetch((i + kPrefetch - 1) % kPrefetch, active && step + kPrefetch - 1 < length);
+            fetch((i + kPrefetch - 1) % kPrefetch,
+                  !CHECKED || (active && step + kPrefetch - 1 < length));
             copy_wait<kPrefetch - 1>();
             uint32_t cost[WORDS];
 #pragma unroll
@@ -578,7 +583,7 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
                 const uint32_t value = mad_lo(t, s.one, mad_lo(m2, s.minus_one, cost[k]));
                 r[k] = (FULL || active) ? value : kInf2;
             }
-            if (active && step < length) {
+            if (!CHECKED || (active && step < length)) {
 #pragma unroll
                 for (int c = 0; c < PIECES; ++c) {
                     if constexpr (PIECE == 16)
@@ -615,6 +620,14 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
             }
             j2 = m2 + p2x2;
         }
+    };
+    // Blocks all of whose steps every line of the warp has, with the copies they
+    // start (kPrefetch - 1 steps ahead), run without the checks: all blocks of the
+    // rows and columns but the last, most of each diagonal's.
+    const int shortest = (int)__reduce_min_sync(kFullMask, (unsigned)length);
+    for (int base = 0; base < steps; base += kPrefetch) {
+        if (FULL && base + 2 * kPrefetch - 1 <= shortest) block(base, std::false_type());
+        else block(base, std::true_type());
     }
     copy_wait<0>();
 }

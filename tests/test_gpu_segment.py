@@ -2,6 +2,8 @@
 stateful pipeline test (test/nx_stereo/stage/stateful_pipeline_test.exs),
 full pipelines against the oracle's chain, pairs in flight, refusals, bad
 runs, timing and release."""
+import time
+
 import numpy as np
 import pytest
 
@@ -304,13 +306,21 @@ def test_waits_poll_time_out_and_call_back(ctx):
         tags.append(tag)
         done.set()
 
+    sent_ns = time.monotonic_ns()
     request = ctx.run_async(94, [{"p1": 8.0, "p2": 64.0, "uniqueness": 1.05}],
                             {"left": left, "right": right}, done=callback, tag=77)
     first = request.wait(0)  # may or may not be done already
     assert request.wait(60000)
+    seen_ns = time.monotonic_ns()
     assert request.poll() and (first in (True, False))
     assert done.wait(10) and tags == [77]
     times = request.times_us()
     assert len(times) == 1 and times[0] > 0
+    # The completion time, read from the device's timestamp of the request's done
+    # event, lies between its sending and the host seeing it done (the mapping onto
+    # CLOCK_MONOTONIC is good to a few microseconds), after the member's time.
+    done_ns = request.done_ns()
+    assert sent_ns + times[0] * 1000 - 20_000 <= done_ns <= seen_ns + 20_000
+    assert request.done_ns() == done_ns
     request.free()
     ctx.release(94)
