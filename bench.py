@@ -47,7 +47,7 @@ PATHS_EVERY = 4  # timed steps between those whose path kernel is bracketed by e
 SERVING_CAP = None
 # DRAM bytes (read + write) of one path-aggregation launch on this workload, from
 # an ncu capture of this command (dram__bytes_read.sum + dram__bytes_write.sum).
-PATHS_TRAFFIC_BYTES = 108_585_728 + 349_709_824
+PATHS_TRAFFIC_BYTES = 107_285_504 + 350_222_336
 
 
 def parse():
@@ -355,8 +355,8 @@ def run_ours(args, rank, world, local_rank):
                      "algorithmic_bytes_per_launch": paths_bytes,
                      "avg_launch_ms": round(paths_avg_s * 1000, 4),
                      "traffic": PATHS_TRAFFIC_BYTES,
-                     "limiter": "the latency of each scan-line step with ~8 warps a SM (ncu: "
-                                "issue 59%, integer ALU pipe 54%, FMA pipe 16%, HBM 39%)"},
+                     "limiter": "instruction issue of the scan-line steps with ~8 warps a SM "
+                                "(ncu: issue 59%, integer ALU pipe 55%, FMA pipe 17%, HBM 43%)"},
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "stages_ms_from": "a second run of the same steps with an event between every stage",
         "pipeline_roofline": {"b_alg_per_pair": b_alg,
@@ -474,8 +474,8 @@ def bench_large(torch, ctx):
     pairs = [scene.rectified_pair(1920, 1080, seed=900 + i, rectangles=12, min_disparity=8,
                                   max_disparity=240, sigma=3.0) for i in range(8)]
     out = _plain_and_batched(torch, ctx, shapes, pairs, repeats=3,
-                             tuner_search={"engine": (0, 1), "order": (0, 1),
-                                           "group_pairs": (1, 2)})
+                             tuner_search={"engine": (0, 1), "streams": (1, 2, 8),
+                                           "order": (0, 1), "group_pairs": (1, 2)})
     out["workload"] = "8 pairs 1920x1080, 256 disparities, 8 paths"
     return out
 
