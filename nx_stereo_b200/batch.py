@@ -304,10 +304,14 @@ class Autotuner:
         for _ in range(self.sweeps):
             improved = False
             for name, values in self.search.items():
-                for value in values:
-                    if value == best[name]:
-                        continue
-                    candidate = dict(best, **{name: value})
+                candidates = [dict(best, **{name: value}) for value in values
+                              if value != best[name]]
+                if name == "engine":  # the stream engine, with every stream count searched
+                    candidates = [dict(c, streams=n) for c in candidates
+                                  for n in (self.search.get("streams") or (c["streams"],))
+                                  if c["engine"] == 1] + [c for c in candidates
+                                                           if c["engine"] != 1]
+                for candidate in candidates:
                     try:
                         ms = self.time(plan, candidate)
                     except native.NativeError:  # a combination the plan refuses
