@@ -89,3 +89,39 @@ def test_a_single_pair_queue():
 def test_refusals(shape, tuning, reason):
     with pytest.raises(native.NativeError, match=reason):
         batch.queue([shape], tuning)
+
+
+class _FakePlan:
+    """A plan whose launch time is a given function of its shapes (no GPU)."""
+
+    def __init__(self, tuning, cost):
+        self._tuning, self.cost = dict(tuning), cost
+        self.shapes = []
+
+    @property
+    def tuning(self):
+        return dict(self._tuning)
+
+    def retune(self, **tuning):
+        self._tuning.update(tuning)
+
+
+def test_autotuner_tries_the_stream_engine_with_each_stream_count():
+    # The stream engine is fastest only with one stream: a search one coordinate
+    # at a time from (engine 0, streams 8) reaches it only if the engine's trial
+    # covers every stream count.
+    def cost(t):
+        if t["engine"] == 1:
+            return {1: 10.0, 2: 11.0, 8: 13.0}[t["streams"]]
+        return 12.0 - (0.5 if t["order"] == 1 else 0.0)
+
+    start = {"engine": 0, "streams": 8, "order": 0}
+    plan = _FakePlan(start, cost)
+    tuner = batch.Autotuner(search={"engine": (0, 1), "streams": (1, 2, 8), "order": (0, 1)})
+    tuner.key = lambda p: "a fake plan"  # (the real key names the device)
+    tuner.time = lambda p, t: (p.retune(**t), tuner.trials.append((p.tuning, p.cost(p.tuning))),
+                               p.cost(p.tuning))[-1]
+    tuning, ms = tuner.tune(plan, use_cache=False)
+    assert (tuning["engine"], tuning["streams"], ms) == (1, 1, 10.0)
+    tried = {(t["engine"], t["streams"]) for t, _ in tuner.trials}
+    assert {(1, 1), (1, 2), (1, 8)} <= tried
