@@ -135,7 +135,11 @@ def test_consistency_and_median(native, oracle):
 
 
 CASES = [((64, 48), 64, 3), ((64, 48), 64, 8), ((64, 48), 128, 3), ((64, 48), 128, 8),
-         ((97, 31), 64, 3), ((97, 31), 64, 8), ((97, 31), 128, 3), ((97, 31), 128, 8)]
+         ((97, 31), 64, 3), ((97, 31), 64, 8), ((97, 31), 128, 3), ((97, 31), 128, 8),
+         # the widest image the reference takes (4096) at its least height (7), and the
+         # narrowest (9) at a height of 4096: scan lines of 4096 steps along rows, and
+         # along columns, in the path kernel's blocks of eight
+         ((4096, 7), 64, 8), ((4096, 9), 128, 8), ((9, 4096), 64, 8)]
 
 
 @pytest.mark.parametrize("size,disparities,paths", CASES)

@@ -65,7 +65,7 @@ def test_ordered_costs(native, oracle, span, disparities):
 
 @pytest.mark.parametrize("span", [0, 8, 16])
 @pytest.mark.parametrize("disparities", [16, 64, 96, 128, 192, 256])
-@pytest.mark.parametrize("w,h", [(70, 23), (9, 7), (131, 5), (300, 17)])
+@pytest.mark.parametrize("w,h", [(70, 23), (9, 7), (131, 5), (300, 17), (4096, 7)])
 def test_census_and_costs_in_one_launch(native, oracle, span, disparities, w, h):
     """nxs_census_costs_device_ordered forms the codes in shared memory: its
     costs equal the oracle's census then costs, at widths below, across and
