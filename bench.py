@@ -39,7 +39,7 @@ import numpy as np  # noqa: E402
 METRIC = "pairs/s at 728x544x128 d, 8 paths (full frame-to-depth pipeline)"
 WIDTH, HEIGHT, DISPARITIES, PATHS = 728, 544, 128, 8
 DECIMATION = 4
-KERNELS_PER_STEP = 8  # rectify, census+costs, paths, select, check+median, despeckle, depth, cloud
+KERNELS_PER_STEP = 6  # rectify, census+costs, paths, select, check+median, despeckle+depth+cloud
 PATHS_EVERY = 4  # timed steps between those whose path kernel is bracketed by events
 # At most this many pairs on the device at once in the serving run, oldest
 # arrival first (None: up to every stream's request slots; caps of 4, 8 and 16
@@ -176,8 +176,8 @@ class DevicePipeline:
         # The costs and path volumes in the order the matcher itself keeps them.
         self.span = int(native.load().nxs_matcher_span(DISPARITIES))
 
-    STAGES = ["rectify", "census_costs", "paths", "select", "check_median", "despeckle",
-              "depth", "cloud"]
+    STAGES = ["rectify", "census_costs", "paths", "select", "check_median",
+              "despeckle_depth_cloud"]
 
     def step(self, frames, marks=None):
         """One pair; `marks` (len(STAGES) + 1 CUDA events or None) bracket the
@@ -211,15 +211,11 @@ class DevicePipeline:
         call("nxs_check_median_device", self.selected.data_ptr(), self.keys.data_ptr(), WIDTH,
              HEIGHT, 1, self.disparity.data_ptr(), s)
         mark(5)
-        call("nxs_despeckle_device", self.disparity.data_ptr(), WIDTH, HEIGHT, 12.0, 1.0, 3,
-             self.speckled.data_ptr(), s)
+        call("nxs_despeckle_depth_cloud_device", self.disparity.data_ptr(), WIDTH, HEIGHT, 12.0,
+             1.0, 3, self.focal, self.baseline, DECIMATION, self.cx, self.cy, 0.05, 20.0,
+             self.speckled.data_ptr(), self.depth_mm.data_ptr(), self.depth_m.data_ptr(),
+             self.grid.data_ptr(), self.kept.data_ptr(), s)
         mark(6)
-        call("nxs_depth_device", self.speckled.data_ptr(), WIDTH * HEIGHT, self.focal,
-             self.baseline, self.depth_mm.data_ptr(), self.depth_m.data_ptr(), s)
-        mark(7)
-        call("nxs_cloud_device", self.depth_m.data_ptr(), WIDTH, HEIGHT, DECIMATION, self.focal,
-             self.cx, self.cy, 0.05, 20.0, self.grid.data_ptr(), self.kept.data_ptr(), s)
-        mark(8)
 
 
 def run_ours(args, rank, world, local_rank):

@@ -367,6 +367,18 @@ nxs_status nxs_cloud_device(const float *d_depth_m, uint32_t width, uint32_t hei
                             float nearest_m, float farthest_m, float *d_grid, int32_t *d_kept,
                             void *stream);
 
+/* SpeckleFilter -> Depth -> PointCloud in one launch: the outputs of
+ * nxs_despeckle_device, then nxs_depth_device on its result, then
+ * nxs_cloud_device on that depth, bit for bit (radius 1..5). */
+nxs_status nxs_despeckle_depth_cloud_device(const float *d_disparity, uint32_t width,
+                                            uint32_t height, float min_support, float max_diff,
+                                            uint32_t radius, float focal_length_px,
+                                            float baseline_m, uint32_t decimation, float cx,
+                                            float cy, float nearest_m, float farthest_m,
+                                            float *d_despeckled, uint16_t *d_depth_mm,
+                                            float *d_depth_m, float *d_grid, int32_t *d_kept,
+                                            void *stream);
+
 /* Stage.Quality's sums (lib/nx_stereo/diagnostics.ex:258-271), f32[5]; then
  * previous := disparity. */
 nxs_status nxs_quality_device(const float *d_disparity, float *d_previous, uint32_t width,

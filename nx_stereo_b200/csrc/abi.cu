@@ -764,6 +764,23 @@ extern "C" nxs_status nxs_cloud_device(const float *d_depth_m, uint32_t width, u
                : NXS_OK;
 }
 
+extern "C" nxs_status nxs_despeckle_depth_cloud_device(
+    const float *d_disparity, uint32_t width, uint32_t height, float min_support, float max_diff,
+    uint32_t radius, float focal_length_px, float baseline_m, uint32_t decimation, float cx,
+    float cy, float nearest_m, float farthest_m, float *d_despeckled, uint16_t *d_depth_mm,
+    float *d_depth_m, float *d_grid, int32_t *d_kept, void *stream) {
+    CHECK_SIZE(d_disparity && d_despeckled && d_depth_mm && d_depth_m && d_grid && d_kept &&
+               width > 0 && height > 0 && radius >= 1 && radius <= 5 && decimation >= 1 &&
+               decimation <= width && decimation <= height && d_despeckled != d_disparity);
+    return launch_despeckle_depth_cloud(d_disparity, width, height, min_support, max_diff,
+                                        radius, focal_length_px, baseline_m, decimation, cx, cy,
+                                        nearest_m, farthest_m, d_despeckled, d_depth_mm,
+                                        d_depth_m, d_grid, d_kept,
+                                        static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
 extern "C" nxs_status nxs_quality_device(const float *d_disparity, float *d_previous,
                                          uint32_t width, uint32_t height, float *d_sums,
                                          void *stream) {

@@ -80,6 +80,14 @@ cudaError_t launch_depth(const float *disparity, size_t pixels, float focal_leng
 cudaError_t launch_cloud(const float *depth_m, int width, int height, int decimation,
                          float focal_length_px, float cx, float cy, float nearest_m,
                          float farthest_m, float *grid, int32_t *kept, cudaStream_t stream);
+// launch_despeckle, launch_depth and launch_cloud in one launch (radius 1..5).
+cudaError_t launch_despeckle_depth_cloud(const float *disparity, int width, int height,
+                                         float min_support, float max_diff, int radius,
+                                         float focal_length_px, float baseline_m,
+                                         int decimation, float cx, float cy, float nearest_m,
+                                         float farthest_m, float *despeckled, uint16_t *depth_mm,
+                                         float *depth_m, float *grid, int32_t *kept,
+                                         cudaStream_t stream);
 // column_sums: scratch of 5 * width floats.
 cudaError_t launch_quality(const float *disparity, float *previous, int width, int height,
                            float *column_sums, float *sums, cudaStream_t stream);

@@ -159,14 +159,15 @@ __global__ void __launch_bounds__(kSpeckleX *kSpeckleY)
 // all issued before any is stored.
 constexpr int kSpeckleRun = 4;
 
+// The filtered values of this thread's kSpeckleRun pixels down column x from
+// row y (a 32 x 8 block of such runs; out[k] is pixel (x, y + k)).
 template <int R>
-__global__ void __launch_bounds__(kSpeckleX *kSpeckleY)
-    despeckle_run_kernel(const float *__restrict__ disparity, int width, int height,
-                         float min_support, float max_diff, float *__restrict__ despeckled) {
+__device__ __forceinline__ void despeckle_run(const float *__restrict__ disparity, int width,
+                                              int height, float min_support, float max_diff,
+                                              float (&out)[kSpeckleRun], int &x, int &y) {
     constexpr int TW = kSpeckleX + 2 * R, TH = kSpeckleY * kSpeckleRun + 2 * R;
     constexpr int THREADS = kSpeckleX * kSpeckleY, PER = (TW * TH + THREADS - 1) / THREADS;
     __shared__ float window[TH][TW];
-    follow_previous_grid();
     const int x0 = blockIdx.x * kSpeckleX, y0 = blockIdx.y * kSpeckleY * kSpeckleRun;
     const int tid = threadIdx.y * kSpeckleX + threadIdx.x;
     float v[PER];
@@ -211,15 +212,24 @@ __global__ void __launch_bounds__(kSpeckleX *kSpeckleY)
             }
         }
     }
-    const int x = x0 + tx;
+    x = x0 + tx;
+    y = y0 + top;
 #pragma unroll
-    for (int k = 0; k < kSpeckleRun; ++k) {
-        const int y = y0 + top + k;
-        if (x < width && y < height) {
-            const bool kept = centre[k] > 0.0f && (float)support[k] >= min_support;
-            despeckled[(size_t)y * width + x] = kept ? centre[k] : -1.0f;
-        }
-    }
+    for (int k = 0; k < kSpeckleRun; ++k)
+        out[k] = centre[k] > 0.0f && (float)support[k] >= min_support ? centre[k] : -1.0f;
+}
+
+template <int R>
+__global__ void __launch_bounds__(kSpeckleX *kSpeckleY)
+    despeckle_run_kernel(const float *__restrict__ disparity, int width, int height,
+                         float min_support, float max_diff, float *__restrict__ despeckled) {
+    follow_previous_grid();
+    float out[kSpeckleRun];
+    int x, y;
+    despeckle_run<R>(disparity, width, height, min_support, max_diff, out, x, y);
+#pragma unroll
+    for (int k = 0; k < kSpeckleRun; ++k)
+        if (x < width && y + k < height) despeckled[(size_t)(y + k) * width + x] = out[k];
 }
 
 cudaError_t launch_despeckle(const float *disparity, int width, int height, float min_support,
@@ -277,18 +287,22 @@ cudaError_t launch_temporal(float *disparity, float *previous, float *missed, si
 // ---------------------------------------------------------------- depth
 // lib/nx_stereo/depth.ex:26-32: depth_m = (f * B) / d where d > 0, else 0;
 // depth_mm = round(depth_m * 1000), 0 beyond 65535.
+__device__ __forceinline__ float depth_of(float d, float focal_baseline, uint16_t *mm) {
+    const float metres = d > 0.0f ? fdiv(focal_baseline, d) : 0.0f;
+    const float rounded = roundf(fmul(metres, 1000.0f));
+    *mm = rounded > 65535.0f ? 0 : (uint16_t)(rounded > 0.0f ? rounded : 0.0f);
+    return metres;
+}
+
 __global__ void depth_kernel(const float *__restrict__ disparity, size_t pixels,
                              float focal_length_px, float baseline_m,
                              uint16_t *__restrict__ depth_mm, float *__restrict__ depth_m) {
     follow_previous_grid();
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pixels) return;
-    const float focal_baseline = fmul(focal_length_px, baseline_m);
-    const float d = disparity[i];
-    const float metres = d > 0.0f ? fdiv(focal_baseline, d) : 0.0f;
-    const float rounded = roundf(fmul(metres, 1000.0f));
-    depth_m[i] = metres;
-    depth_mm[i] = rounded > 65535.0f ? 0 : (uint16_t)(rounded > 0.0f ? rounded : 0.0f);
+    uint16_t mm;
+    depth_m[i] = depth_of(disparity[i], fmul(focal_length_px, baseline_m), &mm);
+    depth_mm[i] = mm;
 }
 
 cudaError_t launch_depth(const float *disparity, size_t pixels, float focal_length_px,
@@ -302,6 +316,21 @@ cudaError_t launch_depth(const float *disparity, size_t pixels, float focal_leng
 // ---------------------------------------------------------------- cloud
 // lib/nx_stereo/depth.ex:73-89: point (i, j) from pixel (i*dec, j*dec),
 // x = (u - cx) * (z / f), y = (v - cy) * (z / f), NaN outside (near, far).
+__device__ __forceinline__ bool cloud_point(float z, int x, int y, float focal_length_px, float cx,
+                                            float cy, float nearest_m, float farthest_m,
+                                            float *point) {
+    const bool in_range = z > nearest_m && z < farthest_m;
+    if (in_range) {
+        const float z_over_f = fdiv(z, focal_length_px);
+        point[0] = fmul(fsub((float)x, cx), z_over_f);
+        point[1] = fmul(fsub((float)y, cy), z_over_f);
+        point[2] = z;
+    } else {
+        point[0] = point[1] = point[2] = __int_as_float(0x7FC00000);
+    }
+    return in_range;
+}
+
 __global__ void cloud_kernel(const float *__restrict__ depth_m, int width, int grid_width,
                              int grid_height, int decimation, float focal_length_px, float cx,
                              float cy, float nearest_m, float farthest_m,
@@ -313,15 +342,8 @@ __global__ void cloud_kernel(const float *__restrict__ depth_m, int width, int g
     const int x = col * decimation, y = row * decimation;
     const float z = depth_m[(size_t)y * width + x];
     float *point = grid + 3 * ((size_t)row * grid_width + col);
-    const bool in_range = z > nearest_m && z < farthest_m;
-    if (in_range) {
-        const float z_over_f = fdiv(z, focal_length_px);
-        point[0] = fmul(fsub((float)x, cx), z_over_f);
-        point[1] = fmul(fsub((float)y, cy), z_over_f);
-        point[2] = z;
-    } else {
-        point[0] = point[1] = point[2] = __int_as_float(0x7FC00000);
-    }
+    const bool in_range = cloud_point(z, x, y, focal_length_px, cx, cy, nearest_m, farthest_m,
+                                      point);
     const unsigned ballot = __ballot_sync(__activemask(), in_range);
     if ((threadIdx.x & 31) == __ffs(__activemask()) - 1 && ballot)
         atomicAdd(kept, (int32_t)__popc(ballot));
@@ -337,6 +359,77 @@ cudaError_t launch_cloud(const float *depth_m, int width, int height, int decima
     dim3 grid_dim((gw + 127) / 128, gh);
     return launch_after(cloud_kernel, grid_dim, dim3(128), 0, stream, depth_m, width, gw, gh,
                         decimation, focal_length_px, cx, cy, nearest_m, farthest_m, grid, kept);
+}
+
+// ---------------------------------------------------------------- despeckle + depth + cloud
+// SpeckleFilter -> Depth -> PointCloud in one launch: each thread filters its
+// run of pixels as despeckle_run_kernel does, then writes their depth as
+// depth_kernel does and, for those on the decimated grid, their point as
+// cloud_kernel does (the same f32 steps on the same values, so the outputs are
+// the three kernels' bit for bit); a warp adds its kept points to *kept at once.
+template <int R>
+__global__ void __launch_bounds__(kSpeckleX *kSpeckleY)
+    despeckle_depth_cloud_kernel(const float *__restrict__ disparity, int width, int height,
+                                 float min_support, float max_diff, float focal_length_px,
+                                 float baseline_m, int decimation, int grid_width,
+                                 int grid_height, float cx, float cy, float nearest_m,
+                                 float farthest_m, float *__restrict__ despeckled,
+                                 uint16_t *__restrict__ depth_mm, float *__restrict__ depth_m,
+                                 float *__restrict__ grid, int32_t *__restrict__ kept) {
+    follow_previous_grid();
+    float out[kSpeckleRun];
+    int x, y;
+    despeckle_run<R>(disparity, width, height, min_support, max_diff, out, x, y);
+    const float focal_baseline = fmul(focal_length_px, baseline_m);
+    const bool on_column = x % decimation == 0 && x / decimation < grid_width;
+    unsigned points = 0;
+#pragma unroll
+    for (int k = 0; k < kSpeckleRun; ++k) {
+        const int yk = y + k;
+        if (x >= width || yk >= height) continue;
+        const size_t i = (size_t)yk * width + x;
+        uint16_t mm;
+        const float metres = depth_of(out[k], focal_baseline, &mm);
+        despeckled[i] = out[k];
+        depth_m[i] = metres;
+        depth_mm[i] = mm;
+        if (on_column && yk % decimation == 0 && yk / decimation < grid_height) {
+            const int row = yk / decimation, col = x / decimation;
+            points += cloud_point(metres, x, yk, focal_length_px, cx, cy, nearest_m, farthest_m,
+                                  grid + 3 * ((size_t)row * grid_width + col));
+        }
+    }
+    points = __reduce_add_sync(kFullMask, points);
+    if ((threadIdx.x & 31) == 0 && points) atomicAdd(kept, (int32_t)points);
+}
+
+cudaError_t launch_despeckle_depth_cloud(const float *disparity, int width, int height,
+                                         float min_support, float max_diff, int radius,
+                                         float focal_length_px, float baseline_m,
+                                         int decimation, float cx, float cy, float nearest_m,
+                                         float farthest_m, float *despeckled, uint16_t *depth_mm,
+                                         float *depth_m, float *grid, int32_t *kept,
+                                         cudaStream_t stream) {
+    if (radius < 1 || radius > 5 || decimation < 1) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(kept, 0, sizeof(int32_t), stream);
+    if (e) return e;
+    const int gw = width / decimation, gh = height / decimation;
+    dim3 block(kSpeckleX, kSpeckleY);
+    dim3 runs((width + kSpeckleX - 1) / kSpeckleX,
+              (height + kSpeckleY * kSpeckleRun - 1) / (kSpeckleY * kSpeckleRun));
+#define NXS_TAIL(R)                                                                           \
+    return launch_after(despeckle_depth_cloud_kernel<R>, runs, block, 0, stream, disparity,   \
+                        width, height, min_support, max_diff, focal_length_px, baseline_m,    \
+                        decimation, gw, gh, cx, cy, nearest_m, farthest_m, despeckled,        \
+                        depth_mm, depth_m, grid, kept)
+    switch (radius) {
+    case 1: NXS_TAIL(1);
+    case 2: NXS_TAIL(2);
+    case 3: NXS_TAIL(3);
+    case 4: NXS_TAIL(4);
+    default: NXS_TAIL(5);
+    }
+#undef NXS_TAIL
 }
 
 // ---------------------------------------------------------------- quality

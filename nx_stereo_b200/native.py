@@ -141,6 +141,8 @@ SIGNATURES = {
     "nxs_temporal_device": (_i, [_P, _P, _P, _u64, _f, _f, _f, _f, _P]),
     "nxs_depth_device": (_i, [_P, _u64, _f, _f, _P, _P, _P]),
     "nxs_cloud_device": (_i, [_P, _u32, _u32, _u32, _f, _f, _f, _f, _f, _P, _P, _P]),
+    "nxs_despeckle_depth_cloud_device": (_i, [_P, _u32, _u32, _f, _f, _u32, _f, _f, _u32, _f,
+                                              _f, _f, _f, _P, _P, _P, _P, _P, _P]),
     "nxs_quality_device": (_i, [_P, _P, _u32, _u32, _P, _P]),
     "nxs_batch_default_tuning": (None, [ctypes.POINTER(BatchTuning)]),
     "nxs_batch_create": (_i, [_P, _u32, ctypes.POINTER(BatchPair), ctypes.POINTER(BatchTuning),

@@ -150,6 +150,44 @@ def test_depth_and_cloud_are_bit_exact(native, oracle):
         assert g.same_bits(grid[finite], want_grid[finite])
 
 
+@pytest.mark.parametrize("radius", [1, 3, 5])
+@pytest.mark.parametrize("size,decimation", [((182 * 4, 136 * 4), 4), ((97, 131), 3),
+                                             ((33, 7), 1), ((4096, 9), 4), ((5, 40), 5)])
+def test_despeckle_depth_cloud_in_one_launch(native, oracle, radius, size, decimation):
+    """nxs_despeckle_depth_cloud_device equals the oracle's despeckle, then depth on
+    its result, then the point cloud of that depth, bit for bit (NaN where no point)."""
+    torch = g.torch()
+    w, h = size
+    rng = np.random.default_rng(w + radius)
+    d = random_disparity(rng, h, w)
+    d[0, :5] = [10.0, 0.0, -1.0, 0.0001, 0.36622][:min(5, w)]
+    speckled = oracle.despeckle(d, 12, 1.0, radius)
+    want_mm, want_m = oracle.depth(speckled, 873.0, 0.2)
+    want_grid, want_kept = oracle.cloud(want_m, decimation, 873.0, w / 2, h / 2, 0.05, 20.0)
+    d_in = g.dev(d)
+    out = {"speckled": g.empty((h, w), torch.float32), "mm": g.empty((h, w), torch.int16),
+           "m": g.empty((h, w), torch.float32),
+           "grid": g.empty(want_grid.shape, torch.float32), "kept": g.empty((1,), torch.int32)}
+    out["kept"].fill_(77)  # the launch zeroes the count before adding to it
+    native.call("nxs_despeckle_depth_cloud_device", g.ptr(d_in), w, h, 12.0, 1.0, radius, 873.0,
+                0.2, decimation, w / 2, h / 2, 0.05, 20.0, g.ptr(out["speckled"]),
+                g.ptr(out["mm"]), g.ptr(out["m"]), g.ptr(out["grid"]), g.ptr(out["kept"]),
+                g.stream())
+    assert g.same_bits(g.host(out["speckled"]), speckled)
+    assert (g.host(out["mm"]).view(np.uint16) == want_mm).all()
+    assert g.same_bits(g.host(out["m"]), want_m)
+    grid = g.host(out["grid"])
+    assert int(g.host(out["kept"])[0]) == want_kept
+    assert (np.isnan(grid) == np.isnan(want_grid)).all()
+    finite = ~np.isnan(want_grid)
+    assert g.same_bits(grid[finite], want_grid[finite])
+    with pytest.raises(native.NativeError):  # the radii compiled in are 1..5
+        native.call("nxs_despeckle_depth_cloud_device", g.ptr(d_in), w, h, 12.0, 1.0, 6, 873.0,
+                    0.2, decimation, w / 2, h / 2, 0.05, 20.0, g.ptr(out["speckled"]),
+                    g.ptr(out["mm"]), g.ptr(out["m"]), g.ptr(out["grid"]), g.ptr(out["kept"]),
+                    g.stream())
+
+
 def test_quality_sums(native, oracle):
     rng = np.random.default_rng(6)
     h, w = 544, 728
