@@ -3,8 +3,8 @@
 // direct entry points.
 //
 // A segment owns its CUDA streams (upload, one or two compute streams,
-// download, and a notify stream for the completion stamps and callbacks), a
-// ring of per-request device slots and what its stages carry from pair to pair (the
+// download, and a notify stream for the callers' completion callbacks), a ring
+// of per-request device slots and what its stages carry from pair to pair (the
 // temporal filter's previous disparity and missed counts, the quality
 // stage's previous disparity). A request copies its entries into pinned
 // memory, enqueues the upload into its slot, every member's kernels and the
