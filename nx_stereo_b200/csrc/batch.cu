@@ -583,12 +583,9 @@ void fork_chains(nxs_batch *b) {
         const nxs_batch_pair &s = b->specs[i];
         const BatchPair &P = b->pairs[i];
         MatcherScratch scratch;
-        scratch.left_codes = P.left_codes;
-        scratch.right_codes = P.right_codes;
         scratch.costs = P.costs;
         scratch.paths = P.paths;
         scratch.selected = P.raw;
-        scratch.checked = P.checked;
         scratch.keys = P.right_map;
         run_matcher(P.left, P.right, (int)s.width, (int)s.height, (int)s.params.disparities,
                     (int)s.params.paths, (int)s.params.p1, (int)s.params.p2, s.params.uniqueness,

@@ -3,10 +3,11 @@
 // left-right check and the median.
 //
 // Layout in HBM for a W x H pair and D disparities (D a multiple of 16):
-//   codes      u64 [2][H][W]     48-bit census codes of both images
-//   costs      u8  [H][W][D]     Hamming costs, 0..48
+//   costs      u8  [H][W][D]     Hamming costs, 0..48 (the census codes of both
+//                                images stay in the census + costs kernel's
+//                                shared memory)
 //   paths      u8  [P][H][W][D]  each direction's path costs, 0..p2+48 <= 127
-//   selected   f32 [H][W], keys u32 [H][W], checked f32 [H][W]
+//   selected   f32 [H][W], keys u32 [H][W]
 // Disparities are the fastest axis so that one scan-line step reads and
 // writes D contiguous bytes: one coalesced 128-byte transaction per warp at
 // D = 128.
@@ -437,25 +438,18 @@ static size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
 size_t matcher_scratch_bytes(int width, int height, int disparities) {
     const size_t pixels = (size_t)width * height, volume = pixels * disparities;
-    return 2 * align256(8 * pixels) + align256(volume) + 8 * align256(volume) +
-           3 * align256(4 * pixels);
+    return align256(volume) + 8 * align256(volume) + 2 * align256(4 * pixels);
 }
 
 MatcherScratch carve_matcher_scratch(void *base, int width, int height, int disparities) {
     const size_t pixels = (size_t)width * height, volume = pixels * disparities;
     char *at = static_cast<char *>(base);
     MatcherScratch s;
-    s.left_codes = reinterpret_cast<uint64_t *>(at);
-    at += align256(8 * pixels);
-    s.right_codes = reinterpret_cast<uint64_t *>(at);
-    at += align256(8 * pixels);
     s.costs = reinterpret_cast<uint8_t *>(at);
     at += align256(volume);
     s.paths = reinterpret_cast<uint8_t *>(at);
     at += 8 * align256(volume);
     s.selected = reinterpret_cast<float *>(at);
-    at += align256(4 * pixels);
-    s.checked = reinterpret_cast<float *>(at);
     at += align256(4 * pixels);
     s.keys = reinterpret_cast<uint32_t *>(at);
     return s;

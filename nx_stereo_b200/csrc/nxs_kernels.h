@@ -92,12 +92,13 @@ cudaError_t launch_despeckle_depth_cloud(const float *disparity, int width, int 
 cudaError_t launch_quality(const float *disparity, float *previous, int width, int height,
                            float *column_sums, float *sums, cudaStream_t stream);
 
-// The matcher's device scratch for one pair, and its layout.
+// The matcher's device scratch for one pair, and its layout: the cost volume,
+// the path volumes, and selection's disparities and keys (the census codes stay
+// in shared memory; the check and median write the output).
 struct MatcherScratch {
-    uint64_t *left_codes, *right_codes;
     uint8_t *costs;
     uint8_t *paths;
-    float *selected, *checked;
+    float *selected;
     uint32_t *keys;
 };
 size_t matcher_scratch_bytes(int width, int height, int disparities);
