@@ -1,11 +1,13 @@
-"""Generates tests/golden/sgm_fixtures.npz from the CPU oracle.
+"""Generates tests/golden/sgm_fixtures.npz: the oracle's own outputs, frozen.
 
-Inputs are the reference's own test images (the xorshift `scene` and `noise`
-generators of native/stereo_match/src/lib.rs:447-508) at the sizes its
-differential tests use (lib.rs:535-593). The oracle is pinned to the
-reference's known answers by tests/test_oracle_known_answers.py; these
-fixtures freeze its outputs so the CUDA path is checked against committed
-data as well as against the live oracle.
+These are regression fixtures of the oracle, not outputs of the reference:
+the reference's own outputs are tests/golden/reference_sgm.npz (made by
+make_reference_fixtures.py from the reference's shader sources). Inputs are
+the reference's test images (the xorshift `scene` and `noise` generators of
+native/stereo_match/src/lib.rs:447-508) at the sizes its differential tests
+use (lib.rs:535-593); freezing the oracle's outputs on them checks the CUDA
+path against committed data as well as against the live oracle, and shows
+any later change of the oracle.
 
     python tests/golden/make_golden.py
 """

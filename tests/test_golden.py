@@ -1,7 +1,8 @@
-"""The committed golden fixtures (tests/golden/sgm_fixtures.npz, made by
-tests/golden/make_golden.py from the oracle on the reference's test images):
-the oracle still reproduces them (CPU), and the CUDA path equals them bit for
-bit (GPU)."""
+"""The oracle's frozen regression fixtures (tests/golden/sgm_fixtures.npz,
+made by tests/golden/make_golden.py from the oracle on the reference's test
+images; the reference's own outputs are checked in test_reference_pin.py and
+test_gpu_reference.py): the oracle still reproduces them (CPU), and the CUDA
+path equals them bit for bit (GPU)."""
 import hashlib
 import os
 
