@@ -221,10 +221,14 @@ nxs_status nxs_sgm_device(nxs_context *context, const uint8_t *d_left, const uin
  * the library, held on every device that loads it until the process exits.
  * Pairs needing more scratch than that (nxs_sgm_scratch_bytes; about 7 million
  * pixel-disparities, e.g. 364x272 at 64) are refused with NXS_BAD_ARGUMENT.
- * The first call on a device finds the array's device address (and loads it
- * there); make that first call before any stream capture. All calls on a
- * device share the array: calls that overlap on the device race, so the
- * caller serialises them. No context is needed and none is used. */
+ * The call works on the calling thread's current device (cudaGetDevice), and
+ * `stream` must belong to that device. The first call on a device finds the
+ * array's device address (and loads it there); make that first call before
+ * any stream capture. The address is kept for the process: after a
+ * cudaDeviceReset of that device, this entry point must not be used again.
+ * All calls on a device share the array: calls that overlap on the device
+ * race, so the caller serialises them. No context is needed and none is
+ * used. */
 nxs_status nxs_sgm_device_static(const uint8_t *d_left, const uint8_t *d_right, uint32_t width,
                                  uint32_t height, const nxs_sgm_params *params,
                                  float *d_disparity, void *stream, char *error,
@@ -415,6 +419,9 @@ typedef struct {
                                single-pair kernels as a chain on one of `streams` streams,
                                the chains overlapping (both in one CUDA graph) */
     int32_t streams;        /* streams of engine 1, 1..64 */
+    uint32_t wait_limit_us; /* engine 0: the longest an item waits for the phase before it,
+                               1..60,000,000 us, after which the launch records a timeout
+                               and ends (NXS_TIMEOUT); 0: 2 s */
 } nxs_batch_tuning;
 
 typedef struct {
@@ -452,6 +459,14 @@ nxs_status nxs_batch_launch(nxs_batch *batch, int32_t host_buffers, void *stream
 
 /* After a launch has finished: NXS_TIMEOUT if a wait inside it ran out. */
 nxs_status nxs_batch_check(nxs_batch *batch, char *error, size_t error_len);
+
+/* For testing the bounded waits of engine 0: plans phase `phase` (1..5, costs
+ * to median) of pair `pair` to wait for one item more of the phase before it
+ * than that phase has, a dependency no launch meets, so every such wait runs
+ * out after wait_limit_us and nxs_batch_run returns NXS_TIMEOUT. The change
+ * is to the device copy of the plan only; nxs_batch_retune plans afresh. */
+nxs_status nxs_batch_hold_phase(nxs_batch *batch, uint32_t pair, uint32_t phase, char *error,
+                                size_t error_len);
 
 nxs_status nxs_batch_info(const nxs_batch *batch, nxs_batch_stats *stats);
 

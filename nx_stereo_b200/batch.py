@@ -22,7 +22,7 @@ from . import native
 
 PHASES = ("census", "costs", "paths", "select", "check", "median")
 TUNING_FIELDS = ("blocks_per_sm", "cost_rows", "select_passes", "group_pairs", "quantum_us",
-                 "order", "path_words", "engine", "streams")
+                 "order", "path_words", "engine", "streams", "wait_limit_us")
 
 
 def default_tuning():
@@ -42,7 +42,7 @@ def _tuning_struct(tuning):
                               int(merged["select_passes"]), int(merged["group_pairs"]),
                               float(merged["quantum_us"]), int(merged["order"]),
                               int(merged["path_words"]), int(merged["engine"]),
-                              int(merged["streams"]))
+                              int(merged["streams"]), int(merged["wait_limit_us"]))
 
 
 def _pairs_struct(shapes):

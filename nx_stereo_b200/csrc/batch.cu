@@ -25,9 +25,10 @@
 // phase k - 1 of that pair is done. Items are taken in queue order and an
 // item only waits on items earlier in the queue, all taken by running blocks,
 // so the earliest unfinished item always runs and the queue cannot deadlock.
-// The wait still has a time limit (kWaitLimitNs), after which the block
+// The wait still has a time limit (the plan's, 2 s by default), after which the block
 // records a timeout in the status word and goes on, so a launch always ends.
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -55,6 +56,7 @@ constexpr int kPixelsPerItem = 1024;   // check and median items
 constexpr int kClocks = 16;
 constexpr int kControlWords = 4 + 2 * kClocks;
 constexpr int kClockWait = kPhases, kClockTake = 2 * kPhases;
+// The default limit of one wait (nxs_batch_tuning.wait_limit_us 0).
 constexpr uint64_t kWaitLimitNs = 2000000000ull;
 
 struct BatchPair {
@@ -133,16 +135,16 @@ __device__ __forceinline__ void select_dispatch(const BatchPair &P, int item, ui
 }
 
 // Waits (thread 0, or lane 0 of a warp) until `*counter` reaches `need`; gives
-// up after kWaitLimitNs and records it in the status word. After one wait has
+// up after `limit_ns` and records it in the status word. After one wait has
 // run out none waits again, so the launch ends instead of waiting out every
 // item.
 __device__ __forceinline__ void wait_for(const unsigned *counter, unsigned need,
-                                         unsigned *control) {
+                                         unsigned *control, uint64_t limit_ns) {
     if (load_acquire(counter) >= need || load_acquire(control + 1)) return;
     const uint64_t start = global_ns();
     while (load_acquire(counter) < need) {
         __nanosleep(256);
-        if (global_ns() - start > kWaitLimitNs) {
+        if (global_ns() - start > limit_ns) {
             atomicOr(control + 1, 1u);
             return;
         }
@@ -157,7 +159,7 @@ template <bool WIDE>
 __device__ __forceinline__ void work(const BatchPair *__restrict__ pairs,
                                      const uint2 *__restrict__ queue, unsigned total,
                                      unsigned *control, uint8_t *smem, PathSetup &setup,
-                                     unsigned long long *clocks) {
+                                     unsigned long long *clocks, uint64_t limit_ns) {
     __shared__ unsigned taken_pair, taken_phase, taken_item, taken_more;
     const int tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
     unsigned *const done = control + kControlWords;
@@ -180,7 +182,7 @@ __device__ __forceinline__ void work(const BatchPair *__restrict__ pairs,
                 clocks[kClockTake] += waiting - taking;
                 if (phase > 0)
                     wait_for(done + pair * kPhases + phase - 1,
-                             (unsigned)pairs[pair].items[phase - 1], control);
+                             (unsigned)pairs[pair].items[phase - 1], control, limit_ns);
                 started = clock64();
                 clocks[kClockWait + phase] += started - waiting;
             }
@@ -285,13 +287,13 @@ __device__ __forceinline__ void work(const BatchPair *__restrict__ pairs,
 template <bool WIDE>
 __global__ void __launch_bounds__(kThreads, WIDE ? 6 : 8)
     batch_kernel(const BatchPair *__restrict__ pairs, const uint2 *__restrict__ queue,
-                 unsigned total, unsigned *control) {
+                 unsigned total, unsigned *control, uint64_t limit_ns) {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ PathSetup setup;
     __shared__ unsigned long long clocks[kClocks];  // this block's cycle sums (thread 0)
     if (threadIdx.x < kClocks) clocks[threadIdx.x] = 0;
     __syncthreads();
-    work<WIDE>(pairs, queue, total, control, smem, setup, clocks);
+    work<WIDE>(pairs, queue, total, control, smem, setup, clocks, limit_ns);
     __syncthreads();
     if (threadIdx.x < kClocks)
         atomicAdd(reinterpret_cast<unsigned long long *>(control + 4) + threadIdx.x,
@@ -306,6 +308,10 @@ void set_error(char *error, size_t error_len, const char *format, ...) {
     va_start(args, format);
     vsnprintf(error, error_len, format, args);
     va_end(args);
+}
+
+uint64_t wait_limit_ns(const nxs_batch_tuning &t) {
+    return t.wait_limit_us ? (uint64_t)t.wait_limit_us * 1000ull : kWaitLimitNs;
 }
 
 nxs_status cuda_failed(cudaError_t e, char *error, size_t error_len, const char *what) {
@@ -565,7 +571,9 @@ void build_runs(const std::vector<nxs_batch_pair> &specs, const std::vector<Batc
 // overlap on the device: one pair's path aggregation (integer-pipe bound, with
 // few warps per SM) beside others' costs (popcount bound) and selection (HBM
 // bound).
-void fork_chains(nxs_batch *b) {
+// Returns the first launch error of the chains (none: cudaSuccess), with the
+// pair it came from in *failed_pair.
+cudaError_t fork_chains(nxs_batch *b, int *failed_pair) {
     const int streams = (int)b->side.size();
     cudaEventRecord(b->fork, b->stream);
     for (cudaStream_t side : b->side) cudaStreamWaitEvent(side, b->fork, 0);
@@ -577,6 +585,7 @@ void fork_chains(nxs_batch *b) {
     };
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work(x) > work(y); });
     std::vector<double> load(streams, 0.0);
+    cudaError_t first = cudaSuccess;
     for (int i : order) {
         const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
         load[k] += work(i);
@@ -587,14 +596,20 @@ void fork_chains(nxs_batch *b) {
         scratch.paths = P.paths;
         scratch.selected = P.raw;
         scratch.keys = P.right_map;
-        run_matcher(P.left, P.right, (int)s.width, (int)s.height, (int)s.params.disparities,
-                    (int)s.params.paths, (int)s.params.p1, (int)s.params.p2, s.params.uniqueness,
-                    s.params.stage_mask ? 1 : 0, scratch, P.disparity, b->side[k]);
+        const cudaError_t e = run_matcher(
+            P.left, P.right, (int)s.width, (int)s.height, (int)s.params.disparities,
+            (int)s.params.paths, (int)s.params.p1, (int)s.params.p2, s.params.uniqueness,
+            s.params.stage_mask ? 1 : 0, scratch, P.disparity, b->side[k]);
+        if (e != cudaSuccess && first == cudaSuccess) {
+            first = e;
+            *failed_pair = i;
+        }
     }
     for (int k = 0; k < streams; ++k) {
         cudaEventRecord(b->joins[k], b->side[k]);
         cudaStreamWaitEvent(b->stream, b->joins[k], 0);
     }
+    return first;
 }
 
 nxs_status capture(nxs_batch *b, bool host, cudaGraphExec_t *out, char *error, size_t error_len) {
@@ -604,18 +619,26 @@ nxs_status capture(nxs_batch *b, bool host, cudaGraphExec_t *out, char *error, s
     if (host)
         cudaMemcpyAsync(b->arena, b->staging, b->input_bytes, cudaMemcpyHostToDevice, b->stream);
     cudaMemsetAsync(b->d_control, 0, b->control_bytes, b->stream);
+    cudaError_t chains = cudaSuccess;
+    int failed_pair = -1;
     if (b->tuning.engine == 1) {
-        fork_chains(b);
+        chains = fork_chains(b, &failed_pair);
     } else {
         auto kernel = b->wide ? batch_kernel<true> : batch_kernel<false>;
         kernel<<<b->grid, kThreads, b->shared_bytes, b->stream>>>(
-            b->d_pairs, b->d_queue, b->total, b->d_control);
+            b->d_pairs, b->d_queue, b->total, b->d_control, wait_limit_ns(b->tuning));
     }
     if (host)
         cudaMemcpyAsync(b->staging + b->input_bytes, b->arena + b->input_bytes, b->output_bytes,
                         cudaMemcpyDeviceToHost, b->stream);
     const cudaError_t launched = cudaGetLastError();
     e = cudaStreamEndCapture(b->stream, &graph);
+    if (chains != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        char where[96];
+        snprintf(where, sizeof where, "capturing the kernels of pair %d", failed_pair);
+        return cuda_failed(chains, error, error_len, where);
+    }
     if (launched) e = launched;
     if (!e) e = cudaGraphInstantiate(out, graph, 0);
     if (graph) cudaGraphDestroy(graph);
@@ -727,11 +750,13 @@ nxs_status check_batch(uint32_t n_pairs, const nxs_batch_pair *specs,
         t.group_pairs > 1024 || !(t.quantum_us > 0.0f && t.quantum_us <= 1000.0f) ||
         (t.order != 0 && t.order != 1) ||
         (t.path_words != 0 && t.path_words != 4 && t.path_words != 8 && t.path_words != 16) ||
-        (t.engine != 0 && t.engine != 1) || t.streams < 1 || t.streams > 64) {
+        (t.engine != 0 && t.engine != 1) || t.streams < 1 || t.streams > 64 ||
+        t.wait_limit_us > 60000000u) {
         set_error(error, error_len,
                   "tuning out of range: blocks_per_sm 1..16, cost_rows 1..64, select_passes "
                   "1..256, group_pairs 1..1024, quantum_us in (0, 1000], order 0 or 1, "
-                  "path_words 0, 4, 8 or 16, engine 0 or 1, streams 1..64");
+                  "path_words 0, 4, 8 or 16, engine 0 or 1, streams 1..64, wait_limit_us "
+                  "0..60000000");
         return NXS_BAD_ARGUMENT;
     }
     for (uint32_t i = 0; i < n_pairs; ++i) {
@@ -759,6 +784,7 @@ extern "C" void nxs_batch_default_tuning(nxs_batch_tuning *t) {
     t->path_words = 0;
     t->engine = 0;
     t->streams = 8;
+    t->wait_limit_us = 0;
 }
 
 extern "C" nxs_status nxs_batch_create(nxs_context *context, uint32_t n_pairs,
@@ -936,8 +962,8 @@ extern "C" nxs_status nxs_batch_run(nxs_batch *b, char *error, size_t error_len)
     if (s) return s;
     const unsigned *control = reinterpret_cast<const unsigned *>(b->staging + b->input_bytes);
     if (control[1]) {
-        set_error(error, error_len, "a batch item waited more than %.1f s for the phase before it",
-                  kWaitLimitNs / 1e9);
+        set_error(error, error_len, "a batch item waited more than %.6f s for the phase before it",
+                  wait_limit_ns(b->tuning) / 1e9);
         return NXS_TIMEOUT;
     }
     return NXS_OK;
@@ -955,11 +981,30 @@ extern "C" nxs_status nxs_batch_check(nxs_batch *b, char *error, size_t error_le
                                error, error_len, "batch status");
     if (s) return s;
     if (status) {
-        set_error(error, error_len, "a batch item waited more than %.1f s for the phase before it",
-                  kWaitLimitNs / 1e9);
+        set_error(error, error_len, "a batch item waited more than %.6f s for the phase before it",
+                  wait_limit_ns(b->tuning) / 1e9);
         return NXS_TIMEOUT;
     }
     return NXS_OK;
+}
+
+extern "C" nxs_status nxs_batch_hold_phase(nxs_batch *b, uint32_t pair, uint32_t phase,
+                                           char *error, size_t error_len) {
+    if (!b || pair >= b->specs.size() || phase < 1 || phase >= (uint32_t)kPhases) {
+        set_error(error, error_len, "a NULL batch, or a pair or phase (1..%d) out of range",
+                  kPhases - 1);
+        return NXS_BAD_ARGUMENT;
+    }
+    std::lock_guard<std::mutex> g(b->lock);
+    cudaSetDevice(b->device);
+    BatchPair held = b->pairs[pair];
+    held.items[phase - 1] += 1;  // one item more than the phase before has: never reached
+    // Only the `items` entry of the device copy changes; the host plan stays.
+    const size_t offset = sizeof(BatchPair) * pair + offsetof(BatchPair, items) +
+                          sizeof(int) * (phase - 1);
+    return cuda_failed(cudaMemcpy(reinterpret_cast<char *>(b->d_pairs) + offset,
+                                  &held.items[phase - 1], sizeof(int), cudaMemcpyHostToDevice),
+                       error, error_len, "batch hold");
 }
 
 extern "C" nxs_status nxs_batch_clocks(nxs_batch *b, uint64_t *cycles) {

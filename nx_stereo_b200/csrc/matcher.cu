@@ -12,6 +12,7 @@
 // writes D contiguous bytes: one coalesced 128-byte transaction per warp at
 // D = 128.
 #include <algorithm>
+#include <mutex>
 
 #include <type_traits>
 
@@ -419,15 +420,33 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// cudaFuncSetAttribute on the current device, once per device ordinal.
+static cudaError_t allow_check_median_shared() {
+    constexpr int kDevices = 64;
+    static std::mutex lock;
+    static bool allowed[kDevices] = {};
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    if (device < 0 || device >= kDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> guard(lock);
+    if (allowed[device]) return cudaSuccess;
+    e = cudaFuncSetAttribute(check_median_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)check_median_shared_bytes(4096));
+    if (e == cudaSuccess) allowed[device] = true;
+    return e;
+}
+
 cudaError_t launch_check_median(const float *disparity, const uint32_t *keys, int width,
                                 int height, int stage_mask, float *filtered,
                                 cudaStream_t stream) {
     const size_t shared = check_median_shared_bytes(width);
-    // Wide images need more than the default 48 KB: allowed once, for the widest.
-    static const cudaError_t allowed = cudaFuncSetAttribute(
-        check_median_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-        (int)check_median_shared_bytes(4096));
-    if (shared > 48 * 1024 && allowed) return allowed;
+    // Wide images need more than the default 48 KB: allowed once per device
+    // (the attribute belongs to the device current when it is set), for the widest.
+    if (shared > 48 * 1024) {
+        const cudaError_t allowed = allow_check_median_shared();
+        if (allowed != cudaSuccess) return allowed;
+    }
     return launch_after(check_median_kernel, dim3((height + kBandRows - 1) / kBandRows),
                         dim3(256), shared, stream, disparity, keys, width, height, stage_mask,
                         filtered);

@@ -1,7 +1,8 @@
 // NxStereo.sgm/3 on device buffers with no device allocation at all: the
-// matcher's scratch (census codes, the cost volume, the path volumes and the
-// per-pixel selection buffers) lives in one fixed array of this file instead of
-// memory obtained from cudaMalloc.
+// matcher's scratch (the cost volume, the path volumes, and the selected
+// disparity and winner keys of each pixel; the census codes never leave the
+// census + costs kernel's shared memory) lives in one fixed array of this file
+// instead of memory obtained from cudaMalloc.
 //
 // Who needs this: callers that must not allocate device memory once running.
 // A caller whose device memory is owned by another allocator (a framework's

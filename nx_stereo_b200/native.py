@@ -81,7 +81,7 @@ class BatchTuning(ctypes.Structure):
                 ("select_passes", ctypes.c_int32), ("group_pairs", ctypes.c_int32),
                 ("quantum_us", ctypes.c_float), ("order", ctypes.c_int32),
                 ("path_words", ctypes.c_int32), ("engine", ctypes.c_int32),
-                ("streams", ctypes.c_int32)]
+                ("streams", ctypes.c_int32), ("wait_limit_us", ctypes.c_uint32)]
 
 
 class BatchStats(ctypes.Structure):
@@ -153,6 +153,7 @@ SIGNATURES = {
     "nxs_batch_run": (_i, [_P] + _err),
     "nxs_batch_launch": (_i, [_P, ctypes.c_int32, _P] + _err),
     "nxs_batch_check": (_i, [_P] + _err),
+    "nxs_batch_hold_phase": (_i, [_P, _u32, _u32] + _err),
     "nxs_batch_info": (_i, [_P, ctypes.POINTER(BatchStats)]),
     "nxs_batch_clocks": (_i, [_P, ctypes.POINTER(_u64)]),
     "nxs_batch_queue": (_i, [_u32, ctypes.POINTER(BatchPair), ctypes.POINTER(BatchTuning),

@@ -125,3 +125,15 @@ def test_autotuner_tries_the_stream_engine_with_each_stream_count():
     assert (tuning["engine"], tuning["streams"], ms) == (1, 1, 10.0)
     tried = {(t["engine"], t["streams"]) for t, _ in tuner.trials}
     assert {(1, 1), (1, 2), (1, 8)} <= tried
+
+
+def test_the_wait_limit_is_a_checked_plan_setting():
+    from nx_stereo_b200 import batch, native
+
+    shapes = [(64, 48, {"disparities": 64})]
+    assert batch.default_tuning()["wait_limit_us"] == 0
+    batch.queue(shapes, {"wait_limit_us": 1000})
+    with pytest.raises(native.NativeError) as raised:
+        batch.queue(shapes, {"wait_limit_us": 60_000_001})
+    assert raised.value.status == native.BAD_ARGUMENT
+    assert "wait_limit_us" in raised.value.message

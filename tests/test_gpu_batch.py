@@ -160,3 +160,34 @@ def test_the_streams_engine_on_the_mixed_batch(ctx):
     for (w, h, s), (left, right), got in zip(MIXED, pairs, plan.run()):
         assert g.same_bits(got, ctx.sgm(left, right, **s)), (w, h, s)
     plan.close()
+
+
+def test_a_dependency_no_launch_meets_times_out_at_the_plans_limit(ctx):
+    """The persistent launch's waits are bounded: with one selection planned
+    to wait for a path item that does not exist, the launch ends after the
+    plan's 1 ms limit (not the 2 s default) with NXS_TIMEOUT, and a fresh
+    plan of the same batch meets every dependency again, results unchanged."""
+    import time
+
+    from nx_stereo_b200 import native
+
+    shapes = [(97, 31, {"disparities": 64}), (64, 48, {"disparities": 64, "paths": 3})]
+    plan = _plan(ctx, shapes, _inputs(shapes, 300), {"engine": 0, "wait_limit_us": 1000})
+    want = plan.run()
+    plan.check()
+    buf = native._errbuf()
+    native._check(native.load().nxs_batch_hold_phase(plan._handle, 1, 3, buf, 1024), buf)
+    started = time.monotonic()
+    with pytest.raises(native.NativeError) as raised:
+        plan.run()
+    assert raised.value.status == native.TIMEOUT
+    assert "0.001000 s" in raised.value.message
+    assert time.monotonic() - started < 1.0
+    with pytest.raises(native.NativeError):
+        plan.check()
+    plan.retune()
+    got = plan.run()
+    plan.check()
+    for a, b in zip(got, want):
+        assert g.same_bits(a, b)
+    plan.close()
