@@ -54,16 +54,31 @@ for _d in (64, 128):
     for _name, (_source, _macros) in BY_DISPARITIES.items():
         MATCHER[f"{_name}_d{_d}"] = (_source, [f"DISPARITIES={_d}"] + _macros)
 
+# The stages' variants (lib/nx_stereo/kernels.ex:19-33) that the segment's
+# stages around the matcher run on a GPU: name -> (source, macros).
+STAGES = {
+    "rectify_bytes": ("rectify", ["WORDS=0"]),
+    "despeckle": ("despeckle", ["RADIUS=3"]),
+    "temporal_filter": ("temporal_filter", ["MAX_MISSED=255"]),
+    "depth": ("depth", []),
+    "point_cloud_rows": ("point_cloud_rows", []),
+    "disparity_rows": ("disparity_rows", []),
+    "column_sums": ("column_sums", []),
+}
+
 VARIANTS = dict(MATCHER)
+VARIANTS.update(STAGES)
 
 _COMMENTS = re.compile(r"//[^\n]*|/\*.*?\*/", re.S)
 _INCLUDE = re.compile(r'^\s*#\s*include\s+"([^"]+)"\s*$', re.M)
-_LOCAL_SIZE = re.compile(r"layout\s*\(\s*local_size_x\s*=\s*([^)]+)\)\s*in\s*;")
-_SPEC = re.compile(r"layout\s*\(\s*constant_id\s*=\s*(\d+)\s*\)\s*const\s+int\s+(\w+)\s*=\s*([^;]+);")
+_LOCAL_SIZE = re.compile(
+    r"layout\s*\(\s*local_size_x\s*=\s*([^,)]+)(?:,\s*local_size_y\s*=\s*([^,)]+))?\s*\)\s*in\s*;")
+_SPEC = re.compile(
+    r"layout\s*\(\s*constant_id\s*=\s*(\d+)\s*\)\s*const\s+(int|float)\s+(\w+)\s*=\s*([^;]+);")
 _BUFFER = re.compile(
     r"layout\s*\(\s*(?:set\s*=\s*\d+\s*,\s*)?binding\s*=\s*(\d+)\s*\)\s*((?:\w+\s+)*?)buffer\s+\w+\s*"
     r"\{\s*(\w+)\s+(\w+)\s*\[\s*[^\]]*\]\s*;\s*\}\s*;")
-_SHARED = re.compile(r"^\s*shared\s+(\w+)\s+(\w+)\s*\[([^\]]+)\]\s*;", re.M)
+_SHARED = re.compile(r"^\s*shared\s+(\w+)\s+(\w+)\s*((?:\[[^\]]+\]\s*)+);", re.M)
 _FLOAT = re.compile(r"(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][-+]?\d+)?|\d+[eE][-+]?\d+)(?![\w.])")
 _SWIZZLE = re.compile(r"\.(xy|zw|xyz|xz|yz)\b(?!\s*\()")
 
@@ -108,19 +123,25 @@ def translate(source, macros):
 
     def local_size(m):
         facts["local_size"] = m.group(1).strip()
-        return "static const int nxs_local_size_x = (%s);" % m.group(1).strip()
+        return "static const int nxs_local_size_x = (%s), nxs_local_size_y = (%s);" % (
+            m.group(1).strip(), (m.group(2) or "1").strip())
 
     def spec(m):
-        facts["spec"].append((int(m.group(1)), m.group(2)))
-        return "int %s = %s;" % (m.group(2), m.group(3).strip())
+        facts["spec"].append((int(m.group(1)), m.group(3), m.group(2) == "float"))
+        return "%s %s = %s;" % (m.group(2), m.group(3), m.group(4).strip())
 
     def buffer(m):
         facts["bindings"].append((int(m.group(1)), m.group(4)))
         return "%s *%s = nullptr;" % (m.group(3), m.group(4))
 
     def shared(m):
-        facts["shared"].append((m.group(1), m.group(2), m.group(3).strip()))
-        return "NXS_SHARED(%s, %s, %s)" % (m.group(1), m.group(2), m.group(3).strip())
+        dims = re.findall(r"\[([^\]]+)\]", m.group(3))
+        if all(re.fullmatch(r"\s*\d+\s*", d) for d in dims):  # sizes fixed by the source
+            return "static %s %s%s;" % (m.group(1), m.group(2), m.group(3))
+        if len(dims) != 1:
+            raise RuntimeError("a shared array of several dimensions sized at run time")
+        facts["shared"].append((m.group(1), m.group(2), dims[0].strip()))
+        return "NXS_SHARED(%s, %s, %s)" % (m.group(1), m.group(2), dims[0].strip())
 
     text = _LOCAL_SIZE.sub(local_size, text)
     text = _SPEC.sub(spec, text)
@@ -139,8 +160,9 @@ def translate(source, macros):
 def emit(name, source, macros):
     text, facts = translate(source, macros)
     ns = "v_" + name
-    spec_ids = ", ".join(str(i) for i, _ in facts["spec"]) or "0"
-    spec_ptrs = ", ".join("&%s::%s" % (ns, n) for _, n in facts["spec"]) or "nullptr"
+    spec_ids = ", ".join(str(i) for i, _, _ in facts["spec"]) or "0"
+    spec_ptrs = ", ".join("(void *)&%s::%s" % (ns, n) for _, n, _ in facts["spec"]) or "nullptr"
+    spec_floats = ", ".join("1" if f else "0" for _, _, f in facts["spec"]) or "0"
     bind_ids = ", ".join(str(b) for b, _ in facts["bindings"]) or "0"
     bind_ptrs = ", ".join("(void **)&%s::%s" % (ns, n) for _, n in facts["bindings"]) or "nullptr"
     checks = "".join(
@@ -157,7 +179,8 @@ static long long nxs_shared_bytes() {{
 }}  // namespace {ns}
 extern "C" const nxs_module *nxs_module_{name}() {{
     static nxs_module m = {{"{name}", &{ns}::shader_main, {ns}::nxs_local_size_x,
-        {len(facts['spec'])}, {{{spec_ids}}}, {{{spec_ptrs}}},
+        {ns}::nxs_local_size_y, {len(facts['spec'])}, {{{spec_ids}}}, {{{spec_ptrs}}},
+        {{{spec_floats}}},
         {len(facts['bindings'])}, {{{bind_ids}}}, {{{bind_ptrs}}}, &{ns}::nxs_shared_bytes}};
     return &m;
 }}

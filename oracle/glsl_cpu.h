@@ -66,6 +66,8 @@ struct vec2 {
     vec2() : x(0), y(0) {}
     explicit vec2(float s) : x(s), y(s) {}
     vec2(float a, float b) : x(a), y(b) {}
+    float &operator[](int i) { return i == 0 ? x : y; }
+    float operator[](int i) const { return i == 0 ? x : y; }
 };
 struct vec3 {
     float x, y, z;
@@ -78,7 +80,24 @@ struct vec4 {
     vec4() : x(0), y(0), z(0), w(0) {}
     explicit vec4(float s) : x(s), y(s), z(s), w(s) {}
     vec4(float a, float b, float c, float d) : x(a), y(b), z(c), w(d) {}
+    float &operator[](int i) { return i == 0 ? x : i == 1 ? y : i == 2 ? z : w; }
+    float operator[](int i) const { return i == 0 ? x : i == 1 ? y : i == 2 ? z : w; }
 };
+/* component-wise arithmetic, each component rounded on its own */
+inline vec2 operator+(vec2 a, vec2 b) { return vec2(a.x + b.x, a.y + b.y); }
+inline vec2 operator-(vec2 a, vec2 b) { return vec2(a.x - b.x, a.y - b.y); }
+inline vec2 operator*(vec2 a, vec2 b) { return vec2(a.x * b.x, a.y * b.y); }
+inline vec2 operator/(vec2 a, vec2 b) { return vec2(a.x / b.x, a.y / b.y); }
+inline vec2 operator*(vec2 a, float b) { return vec2(a.x * b, a.y * b); }
+inline vec2 operator*(float a, vec2 b) { return vec2(a * b.x, a * b.y); }
+inline vec2 operator+(vec2 a, float b) { return vec2(a.x + b, a.y + b); }
+inline vec2 operator-(vec2 a, float b) { return vec2(a.x - b, a.y - b); }
+inline vec2 operator/(vec2 a, float b) { return vec2(a.x / b, a.y / b); }
+inline vec4 operator+(vec4 a, vec4 b) { return vec4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+inline vec4 operator-(vec4 a, vec4 b) { return vec4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
+inline vec4 operator*(vec4 a, vec4 b) { return vec4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w); }
+inline vec4 operator*(vec4 a, float b) { return vec4(a.x * b, a.y * b, a.z * b, a.w * b); }
+inline vec4 operator*(float a, vec4 b) { return vec4(a * b.x, a * b.y, a * b.z, a * b.w); }
 
 /* ---- built-in functions (GLSL 4.50 §8), the overloads the shaders use ---- */
 inline int min(int a, int b) { return a < b ? a : b; }
@@ -119,6 +138,18 @@ inline uint bitfieldExtract(uint v, int offset, int bits) {
     return bits == 0 ? 0u : (v >> offset) & (bits == 32 ? 0xFFFFFFFFu : ((1u << bits) - 1u));
 }
 
+inline vec2 floor(vec2 v) { return vec2(floor(v.x), floor(v.y)); }
+inline vec2 fract(vec2 v) { return vec2(fract(v.x), fract(v.y)); }
+inline vec2 max(vec2 a, vec2 b) { return vec2(max(a.x, b.x), max(a.y, b.y)); }
+inline vec2 min(vec2 a, vec2 b) { return vec2(min(a.x, b.x), min(a.y, b.y)); }
+inline vec2 abs(vec2 v) { return vec2(abs(v.x), abs(v.y)); }
+/* step(edge, x): 0 where x < edge, else 1 */
+inline float step(float edge, float x) { return x < edge ? 0.0f : 1.0f; }
+inline vec2 step(vec2 edge, vec2 x) { return vec2(step(edge.x, x.x), step(edge.y, x.y)); }
+inline vec4 floor(vec4 v) { return vec4(floor(v.x), floor(v.y), floor(v.z), floor(v.w)); }
+inline vec4 max(vec4 a, vec4 b) { return vec4(max(a.x, b.x), max(a.y, b.y), max(a.z, b.z), max(a.w, b.w)); }
+inline vec4 min(vec4 a, vec4 b) { return vec4(min(a.x, b.x), min(a.y, b.y), min(a.z, b.z), min(a.w, b.w)); }
+
 /* atomics on workgroup memory: fibers run one at a time, so a read-modify-write is atomic */
 inline uint atomicMin(uint &mem, uint v) { uint old = mem; mem = min(old, v); return old; }
 inline uint atomicMax(uint &mem, uint v) { uint old = mem; mem = max(old, v); return old; }
@@ -135,6 +166,7 @@ enum nxs_shuffle { NXS_UP = 0, NXS_DOWN = 1, NXS_XOR = 2, NXS_INDEX = 3 };
 
 struct nxs_invocation {
     uvec3 local_id, group_id, global_id;
+    uint local_index;
     uint subgroup_lane, subgroup;
     int state;       /* nxs_sync */
     int op;          /* nxs_shuffle, while state is NXS_SUBGROUP */
@@ -177,25 +209,26 @@ template <typename T> inline T subgroupShuffle(T v, uint index) { return nxs_sub
 #define gl_GlobalInvocationID (nxs_current->global_id)
 #define gl_SubgroupInvocationID (nxs_current->subgroup_lane)
 #define gl_SubgroupID (nxs_current->subgroup)
-#define gl_LocalInvocationIndex (nxs_current->local_id.x)
+#define gl_LocalInvocationIndex (nxs_current->local_index)
 
 /* A shader module as build_ref.py emits it: its entry point, its workgroup
  * size, and where its specialisation constants and buffers live. */
 struct nxs_module {
     const char *name;
     void (*entry)();
-    int local_size_x;
+    int local_size_x, local_size_y;
     int spec_count;
     int spec_id[8];
-    int *spec[8];
+    void *spec[8];
+    int spec_float[8]; /* the constant is a float (else an int) */
     int binding_count;
     int binding[12];
     void **buffer[12];
     long long (*shared_bytes)(); /* bytes its shared arrays need at the current constants */
 };
 
-/* Every workgroup of `groups` in turn, each as local_size_x fibers in
- * subgroups of `subgroup_size`. Returns 0, or -1 with a message in `error`. */
+/* Every workgroup of `groups` in turn, each as local_size_x x local_size_y
+ * fibers (x fastest) in subgroups of `subgroup_size`. Returns 0, or -1 with a message in `error`. */
 extern "C" int nxs_dispatch(const nxs_module *module, uvec3 groups, int subgroup_size, char *error,
                             int error_size);
 

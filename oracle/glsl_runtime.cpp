@@ -110,7 +110,7 @@ extern "C" int nxs_dispatch(const nxs_module *module, uvec3 groups, int subgroup
         std::snprintf(error, error_size, "%s: %s", module->name, what);
         return -1;
     };
-    const int n = module->local_size_x;
+    const int nx = module->local_size_x, n = module->local_size_x * module->local_size_y;
     if (n <= 0 || subgroup_size <= 0 || n % subgroup_size != 0) return fail("bad workgroup size");
     if (module->shared_bytes && module->shared_bytes() < 0)
         return fail("shared arrays exceed the emulator's capacity");
@@ -130,9 +130,12 @@ extern "C" int nxs_dispatch(const nxs_module *module, uvec3 groups, int subgroup
                 for (int i = 0; i < n; ++i) {
                     nxs_invocation &inv = group.invocations[i];
                     std::memset(&inv, 0, sizeof(inv));
-                    inv.local_id = uvec3((uint)i, 0, 0);
+                    const uint lx = (uint)(i % nx), ly = (uint)(i / nx);
+                    inv.local_id = uvec3(lx, ly, 0);
+                    inv.local_index = (uint)i;
                     inv.group_id = uvec3(gx, gy, gz);
-                    inv.global_id = uvec3(gx * (uint)n + (uint)i, gy, gz);
+                    inv.global_id = uvec3(gx * (uint)nx + lx,
+                                          gy * (uint)module->local_size_y + ly, gz);
                     inv.subgroup_lane = (uint)(i % subgroup_size);
                     inv.subgroup = (uint)(i / subgroup_size);
                     inv.state = NXS_RUN;

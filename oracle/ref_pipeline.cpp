@@ -44,7 +44,7 @@ struct Runner {
     // Binds `buffers` to bindings 0, 1, ... and the constants by id, then
     // dispatches `groups` workgroups.
     void run(const std::string &name, uvec3 groups, const std::vector<void *> &buffers,
-             const std::vector<std::pair<int, int>> &constants) {
+             const std::vector<std::pair<int, double>> &constants) {
         if (status) return;
         const nxs_module *m = find(name);
         if (!m) {
@@ -63,7 +63,10 @@ struct Runner {
         }
         for (int i = 0; i < m->spec_count; ++i)
             for (const auto &c : constants)
-                if (c.first == m->spec_id[i]) *m->spec[i] = c.second;
+                if (c.first == m->spec_id[i]) {
+                    if (m->spec_float[i]) *static_cast<float *>(m->spec[i]) = (float)c.second;
+                    else *static_cast<int *>(m->spec[i]) = (int)c.second;
+                }
         status = nxs_dispatch(m, groups, subgroup_size, error, error_size);
     }
 };
@@ -100,7 +103,7 @@ int sgm(const uint8_t *left, const uint8_t *right, int width, int height, int di
     std::vector<uint> forward = volume(), costs = volume(), forward_reverse = volume();
     std::vector<float> disparity(pixels, 0.0f), consistent(pixels, 0.0f);
     std::vector<uint> winners(pixels, 0u);
-    const std::vector<std::pair<int, int>> size = {{0, width}, {1, height}};
+    const std::vector<std::pair<int, double>> size = {{0, width}, {1, height}};
     Runner run{subgroup_size, error, error_size};
 
     // census_stage/3 (vulkan.ex:152-170)
@@ -167,4 +170,116 @@ extern "C" int nxs_ref_sgm(const uint8_t *left, const uint8_t *right, int width,
                            char *error, int error_size) {
     return sgm(left, right, width, height, disparities, paths, p1, p2, uniqueness, output,
                selected, keys, subgroup_size, error, error_size);
+}
+
+/* ---- the stages around the matcher, as lib/nx_stereo/kernels.ex dispatches
+ * their shaders: every buffer a stage reads or writes is bound in the order
+ * its pipeline lists inputs, then outputs; params are the f32 vector
+ * Kernels.scalars/1 makes. */
+
+/* Kernels.rectify/4 for a u8 frame (kernels.ex:49-83: rectify.comp with
+ * WORDS=0, four pixels a thread, the frame read as 32-bit words). `camera`
+ * is k (9), d (5), inverse_pr (9). The image width must be a multiple of 4,
+ * as the shader writes width / 4 words a row. */
+extern "C" int nxs_ref_rectify(const uint8_t *frame, int frame_width, int frame_height,
+                               const float *camera, int width, int height, uint8_t *image,
+                               char *error, int error_size) {
+    if (width % 4 != 0) {
+        std::snprintf(error, error_size, "the shader writes whole words: width %% 4 != 0");
+        return -1;
+    }
+    const size_t frame_bytes = (size_t)frame_width * frame_height;
+    std::vector<uint> words((frame_bytes + 3) / 4, 0u);
+    std::memcpy(words.data(), frame, frame_bytes);
+    std::vector<float> vector(camera, camera + 23);
+    std::vector<uint> packed((size_t)height * (width / 4), 0u);
+    Runner run{32, error, error_size};
+    run.run("rectify_bytes", uvec3(ceil_div((uint)width / 4, 64), (uint)height, 1),
+            {words.data(), vector.data(), packed.data()},
+            {{0, frame_width}, {1, frame_height}, {2, width}, {3, height},
+             {4, (double)((float)frame_width / (float)width)},
+             {5, (double)((float)frame_height / (float)height)}});
+    if (run.status == 0) std::memcpy(image, packed.data(), (size_t)width * height);
+    return run.status;
+}
+
+/* Kernels.despeckle/3 (kernels.ex:114-134): radius 3, params min_support, max_diff. */
+extern "C" int nxs_ref_despeckle(const float *disparity, int width, int height,
+                                 float min_support, float max_diff, float *output, char *error,
+                                 int error_size) {
+    float params[2] = {min_support, max_diff};
+    std::vector<float> in(disparity, disparity + (size_t)width * height);
+    Runner run{32, error, error_size};
+    run.run("despeckle", uvec3(ceil_div((uint)width, 64), ceil_div((uint)height, 16), 1),
+            {in.data(), params, output}, {{0, width}, {1, height}});
+    return run.status;
+}
+
+/* Kernels.temporal_filter/5 (kernels.ex:168-189): params alpha, delta, hold;
+ * a pixel count that is a multiple of 4. */
+extern "C" int nxs_ref_temporal(const float *current, const float *previous, const float *missed,
+                                int pixels, float alpha, float delta, float hold,
+                                float *filtered, float *missed_out, char *error,
+                                int error_size) {
+    if (pixels % 4 != 0) {
+        std::snprintf(error, error_size, "the shader takes whole vec4s: pixels %% 4 != 0");
+        return -1;
+    }
+    float params[3] = {alpha, delta, hold};
+    std::vector<float> c(current, current + pixels), p(previous, previous + pixels),
+        m(missed, missed + pixels);
+    Runner run{32, error, error_size};
+    run.run("temporal_filter", uvec3(ceil_div(ceil_div((uint)pixels, 4), 64), 1, 1),
+            {c.data(), p.data(), m.data(), params, filtered, missed_out}, {{0, pixels}});
+    return run.status;
+}
+
+/* Kernels.depth/3 (kernels.ex:191-212): params focal_length_px, baseline_m;
+ * an even pixel count; millimetres as 16-bit values two a word. */
+extern "C" int nxs_ref_depth(const float *disparity, int pixels, float focal_length_px,
+                             float baseline_m, uint16_t *depth_mm, float *depth_m, char *error,
+                             int error_size) {
+    if (pixels % 2 != 0) {
+        std::snprintf(error, error_size, "the shader takes whole vec2s: pixels %% 2 != 0");
+        return -1;
+    }
+    float params[2] = {focal_length_px, baseline_m};
+    std::vector<float> d(disparity, disparity + pixels);
+    std::vector<uint> mm(pixels / 2, 0u);
+    Runner run{32, error, error_size};
+    run.run("depth", uvec3(ceil_div(ceil_div((uint)pixels, 2), 64), 1, 1),
+            {d.data(), params, mm.data(), depth_m}, {{0, pixels}});
+    if (run.status == 0) std::memcpy(depth_mm, mm.data(), sizeof(uint16_t) * pixels);
+    return run.status;
+}
+
+/* Kernels.point_cloud/4 (kernels.ex:214-245): the grid rows, then the sum of
+ * the rows' kept counts; params focal_length_px, cx, cy, min and max depth. */
+extern "C" int nxs_ref_point_cloud(const float *depth_m, int width, int height, int decimation,
+                                   float focal_length_px, float cx, float cy, float nearest_m,
+                                   float farthest_m, float *grid, float *kept, char *error,
+                                   int error_size) {
+    const int grid_height = height / decimation, grid_width = width / decimation;
+    float params[5] = {focal_length_px, cx, cy, nearest_m, farthest_m};
+    std::vector<float> d(depth_m, depth_m + (size_t)width * height);
+    std::vector<float> rows(grid_height, 0.0f);
+    Runner run{32, error, error_size};
+    run.run("point_cloud_rows", uvec3((uint)grid_height, 1, 1),
+            {d.data(), params, grid, rows.data()},
+            {{0, width}, {1, grid_width}, {2, decimation}});
+    run.run("column_sums", uvec3(1, 1, 1), {rows.data(), kept}, {{0, grid_height}, {1, 1}});
+    return run.status;
+}
+
+/* Kernels.disparity_sums/3 (kernels.ex:247-268): the five sums Stage.Quality
+ * reads, as per-row partial sums added by column. */
+extern "C" int nxs_ref_quality(const float *current, const float *previous, int width,
+                               int height, float *sums, char *error, int error_size) {
+    std::vector<float> c(current, current + (size_t)width * height),
+        p(previous, previous + (size_t)width * height), partials((size_t)height * 5, 0.0f);
+    Runner run{32, error, error_size};
+    run.run("disparity_rows", uvec3((uint)height, 1, 1), {c.data(), p.data(), partials.data()},
+            {{0, width}});
+    run.run("column_sums", uvec3(5, 1, 1), {partials.data(), sums}, {{0, height}, {1, 5}});
+    return run.status;
 }

@@ -23,6 +23,8 @@ this script runs them (oracle/reference_shaders.py) on:
 
 Inputs are seeded (numpy's PCG64 for the noise textures, the bench's own
 scene generator for the scenes) and stored in the file with the outputs.
+tests/golden/reference_stages.npz holds the stages around the matcher the
+same way (stage_fixtures below).
 Needs the reference checkout (to build oracle/_ref); the tests only read the
 committed file.
 
@@ -86,7 +88,55 @@ def fixtures():
     return data
 
 
+def stage_fixtures():
+    """The stages around the matcher as the reference's shaders compute them
+    (lib/nx_stereo/kernels.ex over shaders/rectify.comp, despeckle.comp,
+    temporal_filter.comp, depth.comp, point_cloud_rows.comp,
+    disparity_rows.comp and column_sums.comp), at 364x272 on the frame-to-
+    depth rig: rectification of both raw frames; then, on the reference's own
+    disparity of the rectified pair (with Stage.Disparity's mask), despeckle,
+    a temporal step against a perturbed previous map, depth, the point cloud
+    and the quality sums."""
+    from nx_stereo_b200 import segment
+
+    w, h = 364, 272
+    geometry = segment.standard_geometry(w, h)
+    left, right = scene.rectified_pair(w, h, seed=3, rectangles=6, max_disparity=56)
+    frames = scene.raw_frames(left, right, scene.rig(w, h))
+    data = {"left_frame": frames[0], "right_frame": frames[1]}
+    images = []
+    for side, frame in zip(("left", "right"), frames):
+        c = geometry[side + "_camera"]
+        data[side + "_camera"] = np.concatenate(
+            [np.ravel(c["k"]), np.ravel(c["d"]), np.ravel(c["inverse_pr"])]).astype(np.float32)
+        images.append(reference_shaders.rectify(frame, c["k"], c["d"], c["inverse_pr"], (h, w)))
+        data[side + "_image"] = images[-1]
+    d = reference_shaders.sgm(images[0], images[1], 64, 8, 8, 64, UNIQUENESS)
+    d = np.where(d > 0, d, np.float32(-1.0)).astype(np.float32)
+    data["disparity"] = d
+    data["despeckled"] = reference_shaders.despeckle(d, 12.0, 1.0)
+    rng = np.random.default_rng(17)
+    previous = np.where(rng.random(d.shape) < 0.9,
+                        d + rng.normal(0, 1.5, d.shape).astype(np.float32), -1).astype(np.float32)
+    missed = rng.integers(0, 4, d.shape).astype(np.float32)
+    data["previous"], data["missed"] = previous, missed
+    data["filtered"], data["missed_out"] = reference_shaders.temporal(data["despeckled"], previous,
+                                                                      missed, 0.4, 2.0, 2.0)
+    f, baseline = geometry["focal_length_px"], geometry["baseline_m"]
+    data["depth_mm"], data["depth_m"] = reference_shaders.depth(data["filtered"], f, baseline)
+    cx, cy = geometry["principal_point"]
+    data["cloud_grid"], kept = reference_shaders.point_cloud(data["depth_m"], 4, f, cx, cy, 0.05,
+                                                             20.0)
+    data["cloud_kept"] = np.array(kept, np.int32)
+    data["quality_sums"] = reference_shaders.quality(data["filtered"], previous)
+    data["geometry"] = np.array([f, baseline, cx, cy], np.float32)
+    return data
+
+
 if __name__ == "__main__":
     path = os.path.join(HERE, "reference_sgm.npz")
     np.savez_compressed(path, **fixtures())
+    print(path, os.path.getsize(path), "bytes")
+    path = os.path.join(HERE, "reference_stages.npz")
+    np.savez_compressed(path, **stage_fixtures())
     print(path, os.path.getsize(path), "bytes")

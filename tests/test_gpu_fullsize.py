@@ -30,6 +30,19 @@ def test_728x544_128_disparities_bit_exact(ctx, oracle, paths):
     assert g.same_bits(ctx.sgm(left, right, disparities=128, paths=paths), want)
 
 
+@pytest.mark.parametrize("w,h,d", [(640, 480, 96), (1280, 720, 192)])
+def test_batched_workload_shapes_beyond_the_reference_bit_exact(ctx, oracle, w, h, d):
+    # Two of the batched workload's full-size shapes at disparity counts the
+    # reference refuses (96 and 192), single pairs against the oracle.
+    from nx_stereo_b200 import scene
+
+    left, right = scene.rectified_pair(w, h, seed=w + d, rectangles=6, max_disparity=d - 8)
+    want = oracle.fast_sgm(left, right, d, 8)
+    got = ctx.sgm(left, right, disparities=d, paths=8)
+    assert g.same_bits(got, want)
+    assert (got > 0).mean() > 0.5
+
+
 def test_1920x1080_256_disparities_bit_exact(ctx, oracle):
     from nx_stereo_b200 import scene
 

@@ -140,11 +140,16 @@ def test_disparity_entries_in_either_output_layout(seg_mod, oracle):
 
 
 # ---------------------------------------------------------------- full pipelines vs the oracle
-def _oracle_chain(oracle, geometry, frames, disparities, paths, temporal=None, quality=None):
+def _oracle_chain(oracle, geometry, frames, disparities, paths, temporal=None, quality=None,
+                  fast=False):
     h, w = geometry["height"], geometry["width"]
     images = [oracle.rectify(f, oracle.make_camera(c["k"], c["d"], c["inverse_pr"]), (h, w))
               for f, c in zip(frames, (geometry["left_camera"], geometry["right_camera"]))]
-    d = oracle.disparity_stage(images[0], images[1], disparities, paths)
+    if fast:  # the optimised formulation, then Stage.Disparity's mask (disparity.ex:162)
+        d = oracle.fast_sgm(images[0], images[1], disparities, paths)
+        d = np.where(d > 0, d, np.float32(-1.0)).astype(np.float32)
+    else:
+        d = oracle.disparity_stage(images[0], images[1], disparities, paths)
     d = oracle.despeckle(d, 12, 1.0, 3)
     out = {"left": images[0], "right": images[1]}
     if temporal is not None:
@@ -158,12 +163,13 @@ def _oracle_chain(oracle, geometry, frames, disparities, paths, temporal=None, q
     return out
 
 
-def test_serving_chain_over_several_pairs_matches_the_oracle(seg_mod, oracle):
+@pytest.mark.parametrize("w,h", [(728, 544), (1280, 720)])
+def test_serving_chain_over_several_pairs_matches_the_oracle(seg_mod, oracle, w, h):
     # Rectification -> Disparity(128) -> SpeckleFilter -> TemporalFilter -> Depth -> Quality,
-    # the per-stream chain of the serving workload, on a drifting scene.
+    # the per-stream chain of the serving workload at both of its stream sizes, on
+    # a scene whose surfaces drift from pair to pair, as the serving workload's do.
     from nx_stereo_b200 import scene, stage
 
-    w, h = 728, 544
     geometry = seg_mod.standard_geometry(w, h)
     status, members = seg_mod.members(
         [stage.Rectification, (stage.Disparity, {"num_disparities": 128}), stage.SpeckleFilter,
@@ -174,11 +180,13 @@ def test_serving_chain_over_several_pairs_matches_the_oracle(seg_mod, oracle):
     temporal = {"previous": np.full((h, w), -1.0, np.float32), "missed": np.zeros((h, w), np.float32)}
     quality = {"previous": np.full((h, w), -1.0, np.float32)}
     for k in range(3):
-        left, right = scene.rectified_pair(w, h, seed=40 + k, rectangles=8, max_disparity=120)
+        left, right = scene.rectified_pair(w, h, seed=40, rectangles=8, max_disparity=120,
+                                           frame=k, drift=2.0)
         frames = scene.raw_frames(left, right, rig)
         output, segment_ = run(seg_mod, segment_, {"left_frame": frames[0],
                                                    "right_frame": frames[1]})
-        want = _oracle_chain(oracle, geometry, frames, 128, 8, temporal, quality)
+        want = _oracle_chain(oracle, geometry, frames, 128, 8, temporal, quality,
+                             fast=w > 728)
         for name in ("left", "right", "depth_mm"):
             assert (output[name] == want[name]).all(), name
         assert g.same_bits(output["disparity"], want["disparity"])
