@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 LIBRARY = os.path.join(BUILD, "liboracle.so")
-SOURCES = ["nxs_oracle.c", "nxs_oracle_fast.c"]
+SOURCES = ["nxs_oracle.c", "nxs_oracle_fast.c", "nxs_oracle_band.c"]
 
 
 def build(force=False):

@@ -66,8 +66,46 @@ STAGES = {
     "column_sums": ("column_sums", []),
 }
 
+# The coarse-to-fine search's variants (vulkan.ex:12-77): the shrink and
+# band bases, the dense census windows, and per band width the band's costs,
+# their column-major copy, the scans (a thread a line for bands 8 and 16,
+# band_scan_lanes' lane groups for 32 and 64, whose 8-path form accumulates
+# opposite pairs in band_scan_aggregate) and the selection.
+COARSE_TO_FINE = {
+    "shrink": ("shrink", []),
+    "band_base": ("band_base", []),
+    "census_dense": ("census_dense_pair", []),
+    "census_blend": ("census_dense_pair", ["BLEND=1"]),
+}
+BY_BAND = {
+    "band_cost": ("band_cost", []),
+    "band_transpose_costs": ("band_transpose", []),
+    "band_scan_horizontal": ("band_scan", ["DX=1", "DY=0"]),
+    "band_scan_down": ("band_scan", ["DX=0", "DY=1"]),
+    "band_select": ("band_select", ["PATHS=3"]),
+    "band_select_8": ("band_select", ["PATHS=8"]),
+}
+NARROW_SCANS = {
+    "band_scan_down_up": ("band_scan", ["DX=0", "DY=1", "DX2=0", "DY2=-1"]),
+    "band_scan_down_diagonals": ("band_scan", ["DX=1", "DY=1", "DX2=-1", "DY2=1"]),
+    "band_scan_up_diagonals": ("band_scan", ["DX=1", "DY=-1", "DX2=-1", "DY2=-1"]),
+}
+WIDE_SCANS = {
+    "band_aggregate_vertical": ("band_scan_aggregate", ["DX=0", "DY=1", "FIRST=1"]),
+    "band_aggregate_diagonal": ("band_scan_aggregate", ["DX=1", "DY=1"]),
+    "band_aggregate_antidiagonal": ("band_scan_aggregate", ["DX=-1", "DY=1"]),
+}
+for _band in (8, 16, 32, 64):
+    for _name, (_source, _macros) in {**BY_BAND, **(WIDE_SCANS if _band >= 32 else NARROW_SCANS)}.items():
+        if _source == "band_scan" and _band >= 32:
+            _source = "band_scan_lanes"
+        if _name == "band_select_8" and _band >= 32:
+            _macros = ["AGGREGATED=1"] + _macros
+        COARSE_TO_FINE[f"{_name}_b{_band}"] = (_source, [f"BAND={_band}"] + _macros)
+
 VARIANTS = dict(MATCHER)
 VARIANTS.update(STAGES)
+VARIANTS.update(COARSE_TO_FINE)
 
 _COMMENTS = re.compile(r"//[^\n]*|/\*.*?\*/", re.S)
 _INCLUDE = re.compile(r'^\s*#\s*include\s+"([^"]+)"\s*$', re.M)
@@ -76,8 +114,9 @@ _LOCAL_SIZE = re.compile(
 _SPEC = re.compile(
     r"layout\s*\(\s*constant_id\s*=\s*(\d+)\s*\)\s*const\s+(int|float)\s+(\w+)\s*=\s*([^;]+);")
 _BUFFER = re.compile(
-    r"layout\s*\(\s*(?:set\s*=\s*\d+\s*,\s*)?binding\s*=\s*(\d+)\s*\)\s*((?:\w+\s+)*?)buffer\s+\w+\s*"
+    r"layout\s*\(\s*(?:set\s*=\s*\d+\s*,\s*)?binding\s*=\s*([\d\s+*()-]+?)\s*\)\s*((?:\w+\s+)*?)buffer\s+\w+\s*"
     r"\{\s*(\w+)\s+(\w+)\s*\[\s*[^\]]*\]\s*;\s*\}\s*;")
+_ARRAY_CONSTRUCTOR = re.compile(r"\b(\w+)\s*\[\s*\w*\s*\]\s*\(")
 _SHARED = re.compile(r"^\s*shared\s+(\w+)\s+(\w+)\s*((?:\[[^\]]+\]\s*)+);", re.M)
 _FLOAT = re.compile(r"(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][-+]?\d+)?|\d+[eE][-+]?\d+)(?![\w.])")
 _SWIZZLE = re.compile(r"\.(xy|zw|xyz|xz|yz)\b(?!\s*\()")
@@ -112,6 +151,24 @@ def _parameters(text):
     return text
 
 
+def _array_constructors(text):
+    """GLSL array constructors, T[N](a, b, ...), become brace lists {a, b, ...}
+    (the shaders use them only to initialise a declared array)."""
+    out, at = [], 0
+    for m in _ARRAY_CONSTRUCTOR.finditer(text):
+        if m.start() < at or m.group(1) not in ("uint", "int", "float", "uvec2", "uvec4", "vec2",
+                                                 "vec4", "bool"):
+            continue
+        depth, i = 1, m.end()
+        while depth:
+            depth += {"(": 1, ")": -1}.get(text[i], 0)
+            i += 1
+        out.append(text[at:m.start()] + "{" + text[m.end():i - 1] + "}")
+        at = i
+    out.append(text[at:])
+    return "".join(out)
+
+
 def translate(source, macros):
     """C++ for one shader variant (its source preprocessed with its macros,
     as glslang does); returns (text, module facts)."""
@@ -131,7 +188,11 @@ def translate(source, macros):
         return "%s %s = %s;" % (m.group(2), m.group(3), m.group(4).strip())
 
     def buffer(m):
-        facts["bindings"].append((int(m.group(1)), m.group(4)))
+        # a binding may be a constant expression of the preprocessed source (4 + 1)
+        binding = m.group(1)
+        if not re.fullmatch(r"[\d\s+*()-]+", binding):
+            raise RuntimeError("binding " + binding)
+        facts["bindings"].append((int(eval(binding, {"__builtins__": {}})), m.group(4)))
         return "%s *%s = nullptr;" % (m.group(3), m.group(4))
 
     def shared(m):
@@ -147,6 +208,7 @@ def translate(source, macros):
     text = _SPEC.sub(spec, text)
     text = _BUFFER.sub(buffer, text)
     text = _SHARED.sub(shared, text)
+    text = _array_constructors(text)
     text = _parameters(text)
     text = _SWIZZLE.sub(r".\1()", text)
     text = _FLOAT.sub(lambda m: m.group(1) + "f", text)

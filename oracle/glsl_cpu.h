@@ -30,6 +30,8 @@ struct uvec2 {
     uvec2() : x(0), y(0) {}
     explicit uvec2(uint s) : x(s), y(s) {}
     uvec2(uint a, uint b) : x(a), y(b) {}
+    uint &operator[](int i) { return i == 0 ? x : y; }
+    uint operator[](int i) const { return i == 0 ? x : y; }
 };
 inline uvec2 operator+(uvec2 a, uvec2 b) { return uvec2(a.x + b.x, a.y + b.y); }
 inline uvec2 operator-(uvec2 a, uvec2 b) { return uvec2(a.x - b.x, a.y - b.y); }
@@ -51,8 +53,11 @@ struct uvec4 {
     uvec4(uint a, uint b, uint c, uint d) : x(a), y(b), z(c), w(d) {}
     uvec2 xy() const { return uvec2(x, y); }
     uvec2 zw() const { return uvec2(z, w); }
+    uint &operator[](int i) { return i == 0 ? x : i == 1 ? y : i == 2 ? z : w; }
+    uint operator[](int i) const { return i == 0 ? x : i == 1 ? y : i == 2 ? z : w; }
 };
 inline uvec4 operator+(uvec4 a, uvec4 b) { return uvec4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+inline uvec4 &operator+=(uvec4 &a, uvec4 b) { return a = a + b; }
 
 struct ivec2 {
     int x, y;
@@ -165,8 +170,8 @@ enum nxs_sync { NXS_RUN = 0, NXS_SUBGROUP = 1, NXS_BARRIER = 2, NXS_DONE = 3 };
 enum nxs_shuffle { NXS_UP = 0, NXS_DOWN = 1, NXS_XOR = 2, NXS_INDEX = 3 };
 
 struct nxs_invocation {
-    uvec3 local_id, group_id, global_id;
-    uint local_index;
+    uvec3 local_id, group_id, global_id, groups, group_size;
+    uint local_index, subgroup_size;
     uint subgroup_lane, subgroup;
     int state;       /* nxs_sync */
     int op;          /* nxs_shuffle, while state is NXS_SUBGROUP */
@@ -209,6 +214,9 @@ template <typename T> inline T subgroupShuffle(T v, uint index) { return nxs_sub
 #define gl_GlobalInvocationID (nxs_current->global_id)
 #define gl_SubgroupInvocationID (nxs_current->subgroup_lane)
 #define gl_SubgroupID (nxs_current->subgroup)
+#define gl_SubgroupSize (nxs_current->subgroup_size)
+#define gl_NumWorkGroups (nxs_current->groups)
+#define gl_WorkGroupSize (nxs_current->group_size)
 #define gl_LocalInvocationIndex (nxs_current->local_index)
 
 /* A shader module as build_ref.py emits it: its entry point, its workgroup

@@ -133,6 +133,9 @@ extern "C" int nxs_dispatch(const nxs_module *module, uvec3 groups, int subgroup
                     const uint lx = (uint)(i % nx), ly = (uint)(i / nx);
                     inv.local_id = uvec3(lx, ly, 0);
                     inv.local_index = (uint)i;
+                    inv.groups = groups;
+                    inv.group_size = uvec3((uint)nx, (uint)module->local_size_y, 1);
+                    inv.subgroup_size = (uint)subgroup_size;
                     inv.group_id = uvec3(gx, gy, gz);
                     inv.global_id = uvec3(gx * (uint)nx + lx,
                                           gy * (uint)module->local_size_y + ly, gz);

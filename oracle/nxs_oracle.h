@@ -51,6 +51,32 @@ int oracle_disparity_stage(const uint8_t *left, const uint8_t *right, int width,
                            int disparities, int paths, int p1, int p2, float uniqueness,
                            float *disparity);
 
+/* ---- the coarse-to-fine search (nxs_oracle_band.c) ---- */
+#define ORACLE_SPARSE_9X7 0
+#define ORACLE_DENSE_9X5 1
+#define ORACLE_DENSE_9X5_BLEND 2
+void oracle_census_window(const uint8_t *image, int width, int height, int window,
+                          uint64_t *codes);
+void oracle_shrink(const uint8_t *image, int width, int height, uint8_t *half);
+void oracle_band_base(const float *coarse, int coarse_width, int coarse_height, int band,
+                      int margin, int32_t *base);
+void oracle_band_costs(const uint64_t *left, const uint64_t *right, const int32_t *searched,
+                       int width, int height, int band, int32_t *costs);
+void oracle_band_path(const int32_t *costs, const int32_t *searched, int width, int height,
+                      int band, int dy, int dx, int p1, int p2, int32_t *path);
+void oracle_band_aggregate(const int32_t *costs, const int32_t *searched, int width, int height,
+                           int band, int paths, int p1, int p2, int32_t *sums);
+void oracle_band_select(const int32_t *sums, const int32_t *base, int width, int height, int band,
+                        int disparities, float uniqueness, float *disparity, uint32_t *keys);
+int oracle_sgm_band(const uint8_t *left, const uint8_t *right, const int32_t *base, int width,
+                    int height, int disparities, int paths, int band, int window, int p1, int p2,
+                    float uniqueness, float *disparity);
+/* base_out (may be NULL) receives the band bases of the fine pass. */
+int oracle_sgm_coarse_to_fine(const uint8_t *left, const uint8_t *right, int width, int height,
+                              int paths, int coarse_paths, int band, int margin, int fine_window,
+                              int p1, int p2, float uniqueness, float *disparity,
+                              int32_t *base_out);
+
 /* ---- the stages around the matcher ---- */
 typedef struct {
     float k[9];          /* camera matrix, row-major */

@@ -48,6 +48,16 @@ def lib():
             "oracle_depth": (None, [_f32p, _sz, _f, _f, _u16p, _f32p]),
             "oracle_cloud": (ctypes.c_int32, [_f32p, _i, _i, _i, _f, _f, _f, _f, _f, _f32p]),
             "oracle_quality": (None, [_f32p, _f32p, _i, _i, _f32p]),
+            "oracle_census_window": (None, [_u8p, _i, _i, _i, _u64p]),
+            "oracle_shrink": (None, [_u8p, _i, _i, _u8p]),
+            "oracle_band_base": (None, [_f32p, _i, _i, _i, _i, _i32p]),
+            "oracle_band_costs": (None, [_u64p, _u64p, _i32p, _i, _i, _i, _i32p]),
+            "oracle_band_aggregate": (None, [_i32p, _i32p, _i, _i, _i, _i, _i, _i, _i32p]),
+            "oracle_band_select": (None, [_i32p, _i32p, _i, _i, _i, _i, _f, _f32p, _u32p]),
+            "oracle_sgm_band": (_i, [_u8p, _u8p, _i32p, _i, _i, _i, _i, _i, _i, _i, _i, _f,
+                                     _f32p]),
+            "oracle_sgm_coarse_to_fine": (_i, [_u8p, _u8p, _i, _i, _i, _i, _i, _i, _i, _i, _i,
+                                               _f, _f32p, ctypes.c_void_p]),
             "oracle_noise": (None, [_i, _i, ctypes.c_uint64, _u8p]),
             "oracle_scene": (None, [_i, _i, ctypes.c_uint64, _u8p, _u8p]),
             "oracle_fast_sgm": (_i, [_u8p, _u8p, _i, _i, _i, _i, _i, _i, _f, _f32p]),
@@ -257,3 +267,82 @@ def fast_pipeline_batch(left_frames, right_frames, left_camera, right_camera, si
     if kept < 0:
         raise ValueError("refused")
     return int(kept), out
+
+
+# ---------------------------------------------------------------- coarse to fine
+WINDOWS = {"sparse_9x7": 0, "dense_9x5": 1, "dense_9x5_blend": 2}
+
+
+def census_window(image, window="sparse_9x7"):
+    image = _c(image, np.uint8)
+    h, w = image.shape
+    out = np.empty((h, w), np.uint64)
+    lib().oracle_census_window(image, w, h, WINDOWS[window], out)
+    return out
+
+
+def shrink(image):
+    image = _c(image, np.uint8)
+    h, w = image.shape
+    out = np.empty((h // 2, w // 2), np.uint8)
+    lib().oracle_shrink(image, w, h, out)
+    return out
+
+
+def band_base(coarse, band=16, margin=4):
+    coarse = _c(coarse, np.float32)
+    h, w = coarse.shape
+    out = np.empty((2 * h, 2 * w), np.int32)
+    lib().oracle_band_base(coarse, w, h, band, margin, out)
+    return out
+
+
+def band_costs(left_codes, right_codes, searched, band):
+    h, w = left_codes.shape
+    out = np.empty((h, w, band), np.int32)
+    lib().oracle_band_costs(_c(left_codes, np.uint64), _c(right_codes, np.uint64),
+                            _c(searched, np.int32), w, h, band, out)
+    return out
+
+
+def band_aggregate(costs_, searched, paths, p1, p2):
+    costs_ = _c(costs_, np.int32)
+    h, w, band = costs_.shape
+    out = np.empty_like(costs_)
+    lib().oracle_band_aggregate(costs_, _c(searched, np.int32), w, h, band, paths, p1, p2, out)
+    return out
+
+
+def band_select(sums, base, disparities, uniqueness):
+    sums = _c(sums, np.int32)
+    h, w, band = sums.shape
+    disparity = np.empty((h, w), np.float32)
+    keys = np.empty((h, w), np.uint32)
+    lib().oracle_band_select(sums, _c(base, np.int32), w, h, band, disparities, uniqueness,
+                             disparity, keys)
+    return disparity, keys
+
+
+def sgm_band(left, right, base, disparities=128, paths=8, band=16, census="sparse_9x7", p1=8,
+             p2=64, uniqueness=1.0526315789473684):
+    left, right = _c(left, np.uint8), _c(right, np.uint8)
+    h, w = left.shape
+    out = np.empty((h, w), np.float32)
+    if lib().oracle_sgm_band(left, right, _c(base, np.int32), w, h, disparities, paths, band,
+                             WINDOWS[census], p1, p2, uniqueness, out):
+        raise ValueError("refused")
+    return out
+
+
+def sgm_coarse_to_fine(left, right, paths=8, coarse_paths=None, band=16, margin=4,
+                       fine_census="sparse_9x7", p1=8, p2=64, uniqueness=1.0526315789473684,
+                       with_base=False):
+    left, right = _c(left, np.uint8), _c(right, np.uint8)
+    h, w = left.shape
+    out = np.empty((h, w), np.float32)
+    base = np.empty((h, w), np.int32)
+    if lib().oracle_sgm_coarse_to_fine(left, right, w, h, paths, coarse_paths or paths, band,
+                                       margin, WINDOWS[fine_census], p1, p2, uniqueness, out,
+                                       base.ctypes.data):
+        raise ValueError("refused")
+    return (out, base) if with_base else out

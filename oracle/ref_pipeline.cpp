@@ -283,3 +283,164 @@ extern "C" int nxs_ref_quality(const float *current, const float *previous, int 
     run.run("column_sums", uvec3(5, 1, 1), {partials.data(), sums}, {{0, height}, {1, 5}});
     return run.status;
 }
+
+/* ---- the coarse-to-fine search ---- */
+
+namespace {
+
+// A zero-filled buffer of `words` 32-bit words, with a guard of zero words
+// past its end (the sizes are vulkan.ex's; the guard only keeps a read one
+// past them inside this process's memory).
+std::vector<uint> words_buffer(size_t words) { return std::vector<uint>(words + 256, 0u); }
+
+uvec3 linear_workgroups(uint count) {  // vulkan.ex:257-260
+    const uint rows = ceil_div(count, 65535);
+    return uvec3(ceil_div(count, rows), rows, 1);
+}
+
+}  // namespace
+
+/* NxStereo.Vulkan.band_pipeline/1 (lib/nx_stereo/vulkan.ex:196-255), the
+ * pipeline NxStereo.sgm_band/4 runs on a GPU (lib/nx_stereo.ex:282-321):
+ * `window` 0 sparse 9x7, 1 dense 9x5, 2 dense 9x5 with the blended centre. */
+extern "C" int nxs_ref_sgm_band(const uint8_t *left, const uint8_t *right, const int32_t *base,
+                                int width, int height, int disparities, int paths, int band,
+                                int window, float p1, float p2, float uniqueness, float *output,
+                                int subgroup_size, char *error, int error_size) {
+    if (!(width > 8 && height > 6 && width <= 4096) || (disparities != 64 && disparities != 128) ||
+        (paths != 3 && paths != 8) || !(band == 8 || band == 16 || band == 32 || band == 64) ||
+        window < 0 || window > 2) {
+        std::snprintf(error, error_size, "sizes or settings the reference refuses");
+        return -1;
+    }
+    const uint W = (uint)width, H = (uint)height;
+    const size_t pixels = (size_t)W * H;
+    const size_t tiled_pixels = (size_t)W * ceil_div(H, 8) * 8;
+    const uint cost_words = ceil_div((uint)band * 6, 32);
+    const std::string b = "_b" + std::to_string(band);
+    const uint lines_per_group = band >= 32 ? 64 / (band / 4) : 64;
+    const uint diagonals = W >= H ? W : W + H - 1;
+    std::vector<int> l(pixels), r(pixels), bases(base, base + pixels);
+    for (size_t i = 0; i < pixels; ++i) {
+        l[i] = left[i];
+        r[i] = right[i];
+    }
+    bases.resize(pixels + 256, 0);
+    float params[3] = {p1, p2, uniqueness};
+    std::vector<uint> features = words_buffer(tiled_pixels * 4);
+    std::vector<uint> costs = words_buffer(pixels * cost_words);
+    std::vector<uint> columns = words_buffer(pixels * (cost_words + 1));
+    std::vector<float> disparity(pixels, 0.0f), consistent(pixels, 0.0f);
+    std::vector<uint> winners = words_buffer(pixels);
+    const std::vector<std::pair<int, double>> size = {{0, width}, {1, height}};
+    const std::vector<std::pair<int, double>> with_range = {
+        {0, width}, {1, height}, {2, disparities}};
+    Runner run{subgroup_size, error, error_size};
+    auto lines_of = [&](const char *kind) {
+        return std::string(kind) == "rows" ? H : std::string(kind) == "columns" ? W : diagonals;
+    };
+
+    static const char *census_stage[3] = {"census", "census_dense", "census_blend"};
+    run.run(census_stage[window], uvec3(ceil_div(W, 128 / 8), ceil_div(H, 4 * 8), 1),
+            {l.data(), r.data(), features.data()}, size);
+    run.run("band_cost" + b, uvec3(ceil_div(W, 64), ceil_div(H, 4), 1),
+            {features.data(), bases.data(), costs.data()}, with_range);
+    // the horizontal scans over the column-major copy (vulkan.ex:218-223)
+    std::vector<uint> horizontal = words_buffer(pixels * band / 4);
+    run.run("band_transpose_costs" + b, uvec3(ceil_div(W, 8), ceil_div(H, 8), 1),
+            {costs.data(), bases.data(), columns.data()}, size);
+    run.run("band_scan_horizontal" + b, uvec3(ceil_div(lines_of("rows"), lines_per_group), 1, 1),
+            {params, columns.data(), horizontal.data()}, size);
+    std::vector<std::vector<uint>> volumes;
+    std::vector<void *> select_inputs = {params, bases.data()};
+    if (paths == 8 && band >= 32) {
+        // opposite pairs accumulated into ten-bit sums (vulkan.ex:225-241)
+        const struct {
+            const char *stage, *kind;
+        } wide[3] = {{"band_aggregate_vertical", "columns"},
+                     {"band_aggregate_diagonal", "diagonals"},
+                     {"band_aggregate_antidiagonal", "diagonals"}};
+        void *previous = horizontal.data();
+        for (const auto &w : wide) {
+            volumes.push_back(words_buffer(pixels * band * 10 / 32));
+            run.run(std::string(w.stage) + b,
+                    uvec3(ceil_div(lines_of(w.kind), lines_per_group), 1, 1),
+                    {params, costs.data(), bases.data(), previous, volumes.back().data()}, size);
+            previous = volumes.back().data();
+        }
+        select_inputs.push_back(previous);
+    } else {
+        // @band_scans (vulkan.ex:101-108): {stage, lines, directions}
+        struct Scan {
+            const char *stage, *kind;
+            uint directions;
+        };
+        std::vector<Scan> scans;
+        if (paths == 3) scans = {{"band_scan_down", "columns", 1}};
+        else
+            scans = {{"band_scan_down_up", "columns", 2},
+                     {"band_scan_down_diagonals", "diagonals", 2},
+                     {"band_scan_up_diagonals", "diagonals", 2}};
+        select_inputs.push_back(horizontal.data());
+        volumes.reserve(scans.size());
+        for (const Scan &scan : scans) {
+            volumes.push_back(words_buffer(scan.directions * pixels * band / 4));
+            run.run(std::string(scan.stage) + b,
+                    uvec3(scan.directions * ceil_div(lines_of(scan.kind), lines_per_group), 1, 1),
+                    {params, costs.data(), bases.data(), volumes.back().data()}, size);
+            select_inputs.push_back(volumes.back().data());
+        }
+    }
+    select_inputs.push_back(disparity.data());
+    select_inputs.push_back(winners.data());
+    run.run((paths == 8 ? "band_select_8" : "band_select") + b,
+            linear_workgroups(ceil_div((uint)(pixels * (band / 4)), 64)), select_inputs,
+            with_range);
+    run.run("consistency", uvec3(H, 1, 1), {disparity.data(), winners.data(), consistent.data()},
+            size);
+    run.run("median", uvec3(ceil_div((uint)pixels, 128), 1, 1), {consistent.data(), output}, size);
+    return run.status;
+}
+
+/* NxStereo.sgm_coarse_to_fine/3 (lib/nx_stereo.ex:160-225) as the reference
+ * runs it on a GPU: Vulkan.shrink_pipeline/2, sgm/3's pipeline on the half
+ * pair at 64 disparities, Vulkan.band_base_pipeline/4, then band_pipeline/1
+ * over 128 disparities. `base_out` (may be NULL) receives the bases. */
+extern "C" int nxs_ref_sgm_coarse_to_fine(const uint8_t *left, const uint8_t *right, int width,
+                                          int height, int paths, int coarse_paths, int band,
+                                          int margin, int window, float p1, float p2,
+                                          float uniqueness, float *output, int32_t *base_out,
+                                          int subgroup_size, char *error, int error_size) {
+    if (width % 2 || height % 2) {
+        std::snprintf(error, error_size, "an odd width or height");
+        return -1;
+    }
+    const int hw = width / 2, hh = height / 2;
+    const size_t pixels = (size_t)width * height, half = (size_t)hw * hh;
+    std::vector<int> l(pixels + 256, 0), r(pixels + 256, 0);
+    for (size_t i = 0; i < pixels; ++i) {
+        l[i] = left[i];
+        r[i] = right[i];
+    }
+    std::vector<int> lh(half + 256, 0), rh(half + 256, 0);
+    Runner run{subgroup_size, error, error_size};
+    run.run("shrink", uvec3(ceil_div((uint)half, 64), 1, 1), {l.data(), r.data(), lh.data(), rh.data()},
+            {{0, hw}, {1, hh}});
+    if (run.status) return run.status;
+    std::vector<uint8_t> lb(half), rb(half);
+    for (size_t i = 0; i < half; ++i) {
+        lb[i] = (uint8_t)lh[i];
+        rb[i] = (uint8_t)rh[i];
+    }
+    std::vector<float> coarse(half + 256, 0.0f);
+    int status = sgm(lb.data(), rb.data(), hw, hh, 64, coarse_paths, p1, p2, uniqueness,
+                     coarse.data(), nullptr, nullptr, subgroup_size, error, error_size);
+    if (status) return status;
+    std::vector<int> base(pixels + 256, 0);
+    run.run("band_base", uvec3(ceil_div((uint)half, 64), 1, 1), {coarse.data(), base.data()},
+            {{0, width}, {1, height}, {2, margin}, {3, 128 - band}});
+    if (run.status) return run.status;
+    if (base_out) std::memcpy(base_out, base.data(), sizeof(int32_t) * pixels);
+    return nxs_ref_sgm_band(left, right, base.data(), width, height, 128, paths, band, window, p1,
+                            p2, uniqueness, output, subgroup_size, error, error_size);
+}

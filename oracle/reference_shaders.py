@@ -136,3 +136,38 @@ def quality(current, previous):
     sums = np.zeros(5, np.float32)
     _call("nxs_ref_quality", _p(current), _p(previous), w, h, _p(sums))
     return sums
+
+
+WINDOWS = {"sparse_9x7": 0, "dense_9x5": 1, "dense_9x5_blend": 2}
+
+
+def sgm_band(left, right, base, disparities=128, paths=8, band=16, census="sparse_9x7", p1=8,
+             p2=64, uniqueness=1.0526315789473684, subgroup_size=32):
+    """NxStereo.sgm_band/4 (lib/nx_stereo.ex:282-321) as the reference's band
+    pipeline (lib/nx_stereo/vulkan.ex:196-255) computes it."""
+    left = np.ascontiguousarray(left, np.uint8)
+    right = np.ascontiguousarray(right, np.uint8)
+    base = np.ascontiguousarray(base, np.int32)
+    h, w = left.shape
+    out = np.empty((h, w), np.float32)
+    _call("nxs_ref_sgm_band", _p(left), _p(right), _p(base), w, h, disparities, paths, band,
+          WINDOWS[census], ctypes.c_float(p1), ctypes.c_float(p2), ctypes.c_float(uniqueness),
+          _p(out), subgroup_size)
+    return out
+
+
+def sgm_coarse_to_fine(left, right, paths=8, coarse_paths=None, band=16, margin=4,
+                       fine_census="sparse_9x7", p1=8, p2=64, uniqueness=1.0526315789473684,
+                       subgroup_size=32, with_base=False):
+    """NxStereo.sgm_coarse_to_fine/3 (lib/nx_stereo.ex:160-225) as the
+    reference's shaders compute it: shrink, the coarse sgm/3, the band bases
+    and the band pipeline."""
+    left = np.ascontiguousarray(left, np.uint8)
+    right = np.ascontiguousarray(right, np.uint8)
+    h, w = left.shape
+    out = np.empty((h, w), np.float32)
+    base = np.empty((h, w), np.int32)
+    _call("nxs_ref_sgm_coarse_to_fine", _p(left), _p(right), w, h, paths, coarse_paths or paths,
+          band, margin, WINDOWS[fine_census], ctypes.c_float(p1), ctypes.c_float(p2),
+          ctypes.c_float(uniqueness), _p(out), _p(base), subgroup_size)
+    return (out, base) if with_base else out

@@ -23,8 +23,9 @@ this script runs them (oracle/reference_shaders.py) on:
 
 Inputs are seeded (numpy's PCG64 for the noise textures, the bench's own
 scene generator for the scenes) and stored in the file with the outputs.
-tests/golden/reference_stages.npz holds the stages around the matcher the
-same way (stage_fixtures below).
+tests/golden/reference_stages.npz holds the stages around the matcher and
+tests/golden/reference_band.npz the coarse-to-fine search the same way
+(stage_fixtures and band_fixtures below).
 Needs the reference checkout (to build oracle/_ref); the tests only read the
 committed file.
 
@@ -133,10 +134,79 @@ def stage_fixtures():
     return data
 
 
+def band_fixtures():
+    """The coarse-to-fine search as the reference's shaders compute it
+    (lib/nx_stereo/vulkan.ex:111-255 over shrink.comp, band_base.comp,
+    census_dense_pair.comp, band_cost.comp, band_transpose.comp,
+    band_scan.comp, band_scan_lanes.comp, band_scan_aggregate.comp and
+    band_select.comp):
+
+      - sgm_band/4 at band_bounds_test.exs's shape (19x101 noise textures
+        and a random base in -1..128 - band) for every band and path count,
+        at uniqueness 1.0 as that test sets it;
+      - sgm_band/4 at wide_band_test.exs's shape and bases (18x98; base 0 or
+        128 - band by a phase of the pixel) for bands 32 and 64 at its
+        penalty limits 0/1, 0/79 and 78/79;
+      - the dense census windows (plain and blended) in the fine pass;
+      - sgm_coarse_to_fine/3 on 258x128 unrelated noise halves (the shape of
+        coarse_to_fine_test.exs, 3 coarse paths), on a 364x272 scene and on
+        the 728x544 scene of the frame-to-depth workload (band 16, 8 paths,
+        the reference's fast setting), with their band bases."""
+    data = {}
+    rng = np.random.default_rng(77)
+    for band in (8, 16, 32, 64):
+        for paths in (3, 8):
+            left = rng.integers(0, 256, (19, 101)).astype(np.uint8)
+            right = rng.integers(0, 256, (19, 101)).astype(np.uint8)
+            base = rng.integers(-1, 129 - band, (19, 101)).astype(np.int32)
+            name = f"bounds_b{band}_p{paths}"
+            data.update({name + "/left": left, name + "/right": right, name + "/base": base,
+                         name + "/settings": np.array([band, paths, 8, 64, 0], np.int32),
+                         name + "/uniqueness": np.float32(1.0),
+                         name + "/disparity": reference_shaders.sgm_band(
+                             left, right, base, 128, paths, band, "sparse_9x7", 8, 64, 1.0)})
+    left = rng.integers(0, 256, (18, 98)).astype(np.uint8)
+    right = rng.integers(0, 256, (18, 98)).astype(np.uint8)
+    phase = np.arange(98)[None, :] + 2 * np.arange(18)[:, None]
+    for band in (32, 64):
+        base = np.where(phase % 3 == 0, 0, 128 - band).astype(np.int32)
+        for paths in (3, 8):
+            for p1, p2 in ((0, 1), (0, 79), (78, 79)):
+                name = f"wide_b{band}_p{paths}_{p1}_{p2}"
+                data.update({name + "/left": left, name + "/right": right, name + "/base": base,
+                             name + "/settings": np.array([band, paths, p1, p2, 0], np.int32),
+                             name + "/uniqueness": np.float32(UNIQUENESS),
+                             name + "/disparity": reference_shaders.sgm_band(
+                                 left, right, base, 128, paths, band, "sparse_9x7", p1, p2,
+                                 UNIQUENESS)})
+    texture = rng.integers(0, 256, (128, 516)).astype(np.uint8)
+    halves = (texture[:, :258].copy(), texture[:, 258:].copy())
+    scene364 = scene.rectified_pair(364, 272, seed=21, rectangles=6, max_disparity=120)
+    scene728 = scene.rectified_pair(728, 544, seed=11, rectangles=6, max_disparity=120)
+    runs = [("c2f_noise_258x128_b16_p8_cp3", halves, 16, 8, 3, "sparse_9x7"),
+            ("c2f_scene_364x272_b16_p8", scene364, 16, 8, 8, "sparse_9x7"),
+            ("c2f_scene_364x272_b32_p3", scene364, 32, 3, 3, "sparse_9x7"),
+            ("c2f_scene_364x272_b16_p8_dense", scene364, 16, 8, 8, "dense_9x5"),
+            ("c2f_scene_364x272_b8_p8_blend", scene364, 8, 8, 8, "dense_9x5_blend"),
+            ("c2f_scene_728x544_b16_p8", scene728, 16, 8, 8, "sparse_9x7")]
+    windows = {"sparse_9x7": 0, "dense_9x5": 1, "dense_9x5_blend": 2}
+    for name, (left, right), band, paths, coarse_paths, census in runs:
+        out, base = reference_shaders.sgm_coarse_to_fine(left, right, paths, coarse_paths, band, 4,
+                                                         census, with_base=True)
+        data.update({name + "/left": left, name + "/right": right, name + "/base": base,
+                     name + "/settings": np.array([band, paths, 8, 64, windows[census],
+                                                   coarse_paths, 4], np.int32),
+                     name + "/uniqueness": np.float32(UNIQUENESS), name + "/disparity": out})
+    return data
+
+
 if __name__ == "__main__":
     path = os.path.join(HERE, "reference_sgm.npz")
     np.savez_compressed(path, **fixtures())
     print(path, os.path.getsize(path), "bytes")
     path = os.path.join(HERE, "reference_stages.npz")
     np.savez_compressed(path, **stage_fixtures())
+    print(path, os.path.getsize(path), "bytes")
+    path = os.path.join(HERE, "reference_band.npz")
+    np.savez_compressed(path, **band_fixtures())
     print(path, os.path.getsize(path), "bytes")
