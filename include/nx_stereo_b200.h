@@ -237,6 +237,57 @@ nxs_status nxs_sgm_device_static(const uint8_t *d_left, const uint8_t *d_right, 
 /* The matcher's device scratch, in bytes, for one pair of this size. */
 uint64_t nxs_sgm_scratch_bytes(uint32_t width, uint32_t height, uint32_t disparities);
 
+/* --- the coarse-to-fine search: NxStereo.sgm_coarse_to_fine/3 and
+ * NxStereo.sgm_band/4 (lib/nx_stereo.ex:138-471), Stage.Disparity's
+ * search "coarse_to_fine" (lib/nx_stereo/stage/disparity.ex:140-158) --- */
+typedef struct {
+    nxs_sgm_params sgm;    /* 128 disparities for coarse to fine (as sgm/3 checks the rest) */
+    uint32_t band;         /* candidates a pixel searches: 8, 16, 32 or 64 */
+    uint32_t margin;       /* how far below twice the coarse estimate a band starts, 0..127 */
+    uint32_t coarse_paths; /* the half-size match's paths, 3 or 8 */
+    uint32_t census;       /* the fine census window: 0 sparse 9x7, 1 dense 9x5,
+                              2 dense 9x5 with the blended centre (lib/nx_stereo.ex:491-526) */
+} nxs_band_params;
+
+/* Why sgm_band/4 (coarse_to_fine 0) or sgm_coarse_to_fine/3 (non-zero) would
+ * refuse these settings: sgm/3's checks (nxs_sgm_check) of the pair and, for
+ * coarse to fine, of the half-size pair; the band width and census window;
+ * and for coarse to fine an even width and height and 128 disparities
+ * (lib/nx_stereo.ex:160-183, 300-312). NXS_OK or NXS_BAD_ARGUMENT. */
+nxs_status nxs_band_check(const nxs_band_params *params, uint32_t width, uint32_t height,
+                          int32_t coarse_to_fine, char *error, size_t error_len);
+
+/* NxStereo.sgm_band/4 on device buffers: each pixel searches the disparities
+ * base .. base + band - 1 of d_base (s32 [height][width]; a negative base
+ * marks a pixel with no estimate, searched from 0 and never matched; the
+ * caller keeps base + band within the disparities), enqueued on `stream`
+ * with the context's scratch. */
+nxs_status nxs_sgm_band_device(nxs_context *context, const uint8_t *d_left,
+                               const uint8_t *d_right, const int32_t *d_base, uint32_t width,
+                               uint32_t height, const nxs_band_params *params,
+                               float *d_disparity, void *stream, char *error, size_t error_len);
+
+/* NxStereo.sgm_coarse_to_fine/3 on device buffers: sgm/3 on the pair shrunk
+ * 2x (rounded 2x2 means) at 64 disparities with coarse_paths, each pixel's
+ * band base from it, then sgm_band/4 over 128 disparities; d_base (may be
+ * NULL) receives the bases. With sgm.stage_mask, Stage.Disparity's mask. */
+nxs_status nxs_sgm_coarse_to_fine_device(nxs_context *context, const uint8_t *d_left,
+                                         const uint8_t *d_right, uint32_t width, uint32_t height,
+                                         const nxs_band_params *params, float *d_disparity,
+                                         int32_t *d_base, void *stream, char *error,
+                                         size_t error_len);
+
+/* The same on a pair in host memory. Synchronous. */
+nxs_status nxs_sgm_coarse_to_fine(nxs_context *context, const uint8_t *left,
+                                  const uint8_t *right, uint32_t width, uint32_t height,
+                                  const nxs_band_params *params, float *disparity, char *error,
+                                  size_t error_len);
+
+/* The device scratch, in bytes, of sgm_band/4 (coarse_to_fine 0) or of
+ * sgm_coarse_to_fine/3 for one pair. */
+uint64_t nxs_band_scratch_bytes(uint32_t width, uint32_t height, uint32_t band,
+                                int32_t coarse_to_fine);
+
 /* --- the matcher's steps, for checking intermediates (device buffers) --- */
 
 /* 48-bit 9x7 census codes, u64 per pixel (lib/nx_stereo.ex:491-505). */

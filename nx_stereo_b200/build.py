@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBRARY = os.path.join(HERE, "libnxs_b200.so")
-SOURCES = ["matcher.cu", "stages.cu", "abi.cu", "matcher_static.cu", "batch.cu"]
+SOURCES = ["matcher.cu", "stages.cu", "abi.cu", "matcher_static.cu", "batch.cu", "band.cu"]
 HEADERS = ["nxs_device.cuh", "nxs_kernels.h", "nxs_matcher.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",

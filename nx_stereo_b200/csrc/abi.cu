@@ -218,6 +218,8 @@ struct Member {
     Kind kind;
     std::string kind_name;
     int disparities = 0, paths = 0, radius = 3, decimation = 1;
+    // Disparity's coarse-to-fine search (coarse_to_fine non-zero) and its settings
+    int coarse_to_fine = 0, band = 16, margin = 4, coarse_paths = 8, census = 0;
     float max_missed = 255.0f, min_depth_m = 0.0f, max_depth_m = INFINITY;
     // carried from pair to pair
     float *previous = nullptr, *missed = nullptr;
@@ -500,6 +502,140 @@ extern "C" nxs_status nxs_sgm(nxs_context *c, const uint8_t *left, const uint8_t
     if ((e = cudaMemcpyAsync(disparity, d_out, 4 * pixels, cudaMemcpyDeviceToHost, c->stream)) ||
         (e = cudaStreamSynchronize(c->stream)))
         return cuda_status(e, error, error_len, "matcher");
+    return NXS_OK;
+}
+
+extern "C" nxs_status nxs_band_check(const nxs_band_params *p, uint32_t width, uint32_t height,
+                                     int32_t coarse_to_fine, char *error, size_t error_len) {
+    if (!p) {
+        set_error(error, error_len, "params is NULL");
+        return NXS_BAD_ARGUMENT;
+    }
+    nxs_status s = nxs_sgm_check(&p->sgm, width, height, error, error_len);
+    if (s) return s;
+    // sgm_band/4's band check (lib/nx_stereo.ex:300-304) and census_window!/2 (481-489)
+    if (p->band != 8 && p->band != 16 && p->band != 32 && p->band != 64) {
+        set_error(error, error_len, ":band must be 8, 16, 32 or 64, got %u", p->band);
+        return NXS_BAD_ARGUMENT;
+    }
+    if (p->census > 2) {
+        set_error(error, error_len,
+                  "census must be 0 (sparse 9x7), 1 (dense 9x5) or 2 (dense 9x5 blend), got %u",
+                  p->census);
+        return NXS_BAD_ARGUMENT;
+    }
+    if (!coarse_to_fine) return NXS_OK;
+    // sgm_coarse_to_fine/3's checks (lib/nx_stereo.ex:173-183)
+    if (width % 2 || height % 2) {
+        set_error(error, error_len,
+                  "coarse to fine expects images of even height and width, got %ux%u", width,
+                  height);
+        return NXS_BAD_ARGUMENT;
+    }
+    if (p->sgm.disparities != 128) {
+        set_error(error, error_len,
+                  ":disparities must be 128: the coarse matching takes 64, got %u",
+                  p->sgm.disparities);
+        return NXS_BAD_ARGUMENT;
+    }
+    if (p->coarse_paths != 3 && p->coarse_paths != 8) {
+        set_error(error, error_len, "coarse_paths must be 3 or 8, got %u", p->coarse_paths);
+        return NXS_BAD_ARGUMENT;
+    }
+    if (p->margin > 127) {
+        set_error(error, error_len, "margin must be 0..127, got %u", p->margin);
+        return NXS_BAD_ARGUMENT;
+    }
+    nxs_sgm_params coarse = p->sgm;
+    coarse.disparities = 64;
+    coarse.paths = p->coarse_paths;
+    return nxs_sgm_check(&coarse, width / 2, height / 2, error, error_len);
+}
+
+extern "C" uint64_t nxs_band_scratch_bytes(uint32_t width, uint32_t height, uint32_t band,
+                                           int32_t coarse_to_fine) {
+    return coarse_to_fine ? coarse_to_fine_scratch_bytes(width, height, band)
+                          : band_scratch_bytes(width, height, band);
+}
+
+extern "C" nxs_status nxs_sgm_band_device(nxs_context *c, const uint8_t *d_left,
+                                          const uint8_t *d_right, const int32_t *d_base,
+                                          uint32_t width, uint32_t height,
+                                          const nxs_band_params *p, float *d_disparity,
+                                          void *stream, char *error, size_t error_len) {
+    if (!c || !d_left || !d_right || !d_base || !d_disparity) {
+        set_error(error, error_len, "a NULL context or buffer");
+        return NXS_BAD_ARGUMENT;
+    }
+    nxs_status s = nxs_band_check(p, width, height, 0, error, error_len);
+    if (s) return s;
+    cudaSetDevice(c->device);
+    std::lock_guard<std::mutex> g(c->lock);
+    cudaError_t e = c->scratch.reserve(band_scratch_bytes(width, height, p->band));
+    if (e) return cuda_status(e, error, error_len, "scratch allocation");
+    BandScratch bs = carve_band_scratch(c->scratch.ptr, width, height, p->band);
+    e = run_band_matcher(d_left, d_right, d_base, width, height, p->sgm.disparities, p->sgm.paths,
+                         p->band, p->census, p->sgm.p1, p->sgm.p2, p->sgm.uniqueness,
+                         p->sgm.stage_mask ? 1 : 0, bs, d_disparity,
+                         static_cast<cudaStream_t>(stream));
+    return cuda_status(e, error, error_len, "band matcher launch");
+}
+
+extern "C" nxs_status nxs_sgm_coarse_to_fine_device(nxs_context *c, const uint8_t *d_left,
+                                                    const uint8_t *d_right, uint32_t width,
+                                                    uint32_t height, const nxs_band_params *p,
+                                                    float *d_disparity, int32_t *d_base,
+                                                    void *stream, char *error,
+                                                    size_t error_len) {
+    if (!c || !d_left || !d_right || !d_disparity) {
+        set_error(error, error_len, "a NULL context or buffer");
+        return NXS_BAD_ARGUMENT;
+    }
+    nxs_status s = nxs_band_check(p, width, height, 1, error, error_len);
+    if (s) return s;
+    cudaSetDevice(c->device);
+    std::lock_guard<std::mutex> g(c->lock);
+    cudaError_t e = c->scratch.reserve(coarse_to_fine_scratch_bytes(width, height, p->band));
+    if (e) return cuda_status(e, error, error_len, "scratch allocation");
+    e = run_coarse_to_fine(d_left, d_right, width, height, p->sgm.paths, p->coarse_paths,
+                           p->band, p->margin, p->census, p->sgm.p1, p->sgm.p2,
+                           p->sgm.uniqueness, p->sgm.stage_mask ? 1 : 0, c->scratch.ptr,
+                           d_disparity, d_base, static_cast<cudaStream_t>(stream));
+    return cuda_status(e, error, error_len, "coarse-to-fine launch");
+}
+
+extern "C" nxs_status nxs_sgm_coarse_to_fine(nxs_context *c, const uint8_t *left,
+                                             const uint8_t *right, uint32_t width,
+                                             uint32_t height, const nxs_band_params *p,
+                                             float *disparity, char *error, size_t error_len) {
+    if (!c || !left || !right || !disparity) {
+        set_error(error, error_len, "a NULL context or buffer");
+        return NXS_BAD_ARGUMENT;
+    }
+    nxs_status s = nxs_band_check(p, width, height, 1, error, error_len);
+    if (s) return s;
+    cudaSetDevice(c->device);
+    const size_t pixels = (size_t)width * height, aligned = (pixels + 255) & ~(size_t)255;
+    uint8_t *d_left, *d_right;
+    float *d_out;
+    {
+        std::lock_guard<std::mutex> g(c->lock);
+        cudaError_t e = c->io.reserve(2 * aligned + 4 * pixels);
+        if (e) return cuda_status(e, error, error_len, "buffer allocation");
+        d_left = static_cast<uint8_t *>(c->io.ptr);
+        d_right = d_left + aligned;
+        d_out = reinterpret_cast<float *>(d_right + aligned);
+    }
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(d_left, left, pixels, cudaMemcpyHostToDevice, c->stream)) ||
+        (e = cudaMemcpyAsync(d_right, right, pixels, cudaMemcpyHostToDevice, c->stream)))
+        return cuda_status(e, error, error_len, "copy to the device");
+    s = nxs_sgm_coarse_to_fine_device(c, d_left, d_right, width, height, p, d_out, nullptr,
+                                      c->stream, error, error_len);
+    if (s) return s;
+    if ((e = cudaMemcpyAsync(disparity, d_out, 4 * pixels, cudaMemcpyDeviceToHost, c->stream)) ||
+        (e = cudaStreamSynchronize(c->stream)))
+        return cuda_status(e, error, error_len, "coarse to fine");
     return NXS_OK;
 }
 
@@ -931,13 +1067,36 @@ bool build_member(const nxs_geometry &g, const nxs_member &m, Member *out, std::
         }
         return true;
     case Kind::Disparity: {
-        if (!takes_only(m, {"num_disparities", "paths"}, why)) return false;
+        if (!takes_only(m, {"num_disparities", "paths", "coarse_to_fine", "band", "margin",
+                            "coarse_paths", "fine_census"},
+                        why))
+            return false;
         if (!integer_option(m, "num_disparities", {64, 96, 128, 192, 256}, &out->disparities,
                             why) ||
             !integer_option(m, "paths", {3, 8}, &out->paths, why))
             return false;
         nxs_sgm_params p{(uint32_t)out->disparities, (uint32_t)out->paths, 8, 64, 1.0f, 1};
         char buf[256];
+        if (find_setting(m, "coarse_to_fine")) {
+            // Stage.Disparity's search "coarse_to_fine" (stage/disparity.ex:72-108): the
+            // band, margin, coarse paths and fine census (0 sparse 9x7, 1 dense 9x5, 2 blended)
+            if (!integer_option(m, "coarse_to_fine", {0, 1}, &out->coarse_to_fine, why))
+                return false;
+        }
+        if (out->coarse_to_fine) {
+            if (!integer_option(m, "band", {8, 16, 32, 64}, &out->band, why) ||
+                !count_option(m, "margin", 0, out->band - 1, &out->margin, why) ||
+                !integer_option(m, "coarse_paths", {3, 8}, &out->coarse_paths, why) ||
+                !count_option(m, "fine_census", 0, 2, &out->census, why))
+                return false;
+            nxs_band_params bp{p, (uint32_t)out->band, (uint32_t)out->margin,
+                               (uint32_t)out->coarse_paths, (uint32_t)out->census};
+            if (nxs_band_check(&bp, g.width, g.height, 1, buf, sizeof buf)) {
+                *why = buf;
+                return false;
+            }
+            return true;
+        }
         if (nxs_sgm_check(&p, g.width, g.height, buf, sizeof buf)) {
             *why = buf;
             return false;
@@ -1157,8 +1316,15 @@ extern "C" nxs_status nxs_configure(nxs_context *c, uint32_t id, const nxs_geome
     const size_t pixels = (size_t)g.width * g.height;
     const size_t frame = (size_t)g.frame_width * g.frame_height;
     int max_disparities = 0, decimation = 1;
+    size_t matcher_scratch = 0;  // the largest disparity member's
     for (const Member &m : seg->members) {
-        if (m.kind == Kind::Disparity) max_disparities = std::max(max_disparities, m.disparities);
+        if (m.kind == Kind::Disparity) {
+            max_disparities = std::max(max_disparities, m.disparities);
+            matcher_scratch = std::max(
+                matcher_scratch, m.coarse_to_fine
+                                     ? coarse_to_fine_scratch_bytes(g.width, g.height, m.band)
+                                     : matcher_scratch_bytes(g.width, g.height, m.disparities));
+        }
         if (m.kind == Kind::Cloud) decimation = m.decimation;
     }
     // Each speckle filter moves the disparity to the slot's other buffer.
@@ -1234,8 +1400,7 @@ extern "C" nxs_status nxs_configure(nxs_context *c, uint32_t id, const nxs_geome
     }
     for (int k = 0; k < seg->n_lanes; ++k) {
         if (!e) e = seg->alloc(&seg->depth_m[k], pixels);
-        if (!e && max_disparities)
-            e = seg->scratch[k].reserve(matcher_scratch_bytes(g.width, g.height, max_disparities));
+        if (!e && max_disparities) e = seg->scratch[k].reserve(matcher_scratch);
     }
     if (!e) e = seg->alloc(&seg->quality_columns, 5 * (size_t)g.width);
     // What the stages carry starts over: previous = -1, missed = 0
@@ -1401,6 +1566,13 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
                                     slot.images[0], slot.images[1], s);
             break;
         case Kind::Disparity: {
+            if (m.coarse_to_fine) {
+                e = run_coarse_to_fine(slot.images[0], slot.images[1], g.width, g.height, m.paths,
+                                       m.coarse_paths, m.band, m.margin, m.census, l.sgm.p1,
+                                       l.sgm.p2, l.sgm.uniqueness, 1, seg->scratch[lane].ptr,
+                                       slot.disparity[current], nullptr, s);
+                break;
+            }
             MatcherScratch ms =
                 carve_matcher_scratch(seg->scratch[lane].ptr, g.width, g.height, m.disparities);
             e = run_matcher(slot.images[0], slot.images[1], g.width, g.height, m.disparities,

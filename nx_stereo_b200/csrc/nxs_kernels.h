@@ -111,6 +111,56 @@ cudaError_t run_matcher(const uint8_t *left, const uint8_t *right, int width, in
                         int stage_mask, const MatcherScratch &scratch, float *disparity,
                         cudaStream_t stream);
 
+// ---- the coarse-to-fine search (band.cu) ----
+// Both images' rounded 2x2 means.
+cudaError_t launch_shrink_pair(const uint8_t *left, const uint8_t *right, int width, int height,
+                               uint8_t *left_half, uint8_t *right_half, cudaStream_t stream);
+// Each full-size pixel's band base from the coarse disparity {ch, cw}.
+cudaError_t launch_band_base(const float *coarse, int coarse_width, int coarse_height, int band,
+                             int margin, int32_t *base, cudaStream_t stream);
+// window 0: the sparse 9x7 census (launch_census); 1: dense 9x5; 2: dense 9x5 blended.
+cudaError_t launch_census_window(const uint8_t *left, const uint8_t *right, int width,
+                                 int height, int window, uint64_t *left_codes,
+                                 uint64_t *right_codes, cudaStream_t stream);
+cudaError_t launch_band_costs(const uint64_t *left_codes, const uint64_t *right_codes,
+                              const int32_t *base, int width, int height, int band,
+                              uint8_t *costs, cudaStream_t stream);
+cudaError_t launch_band_paths(const uint8_t *costs, const int32_t *base, int width, int height,
+                              int band, int paths, int p1, int p2, uint8_t *out,
+                              cudaStream_t stream);
+cudaError_t launch_band_select(const uint8_t *paths_in, const int32_t *base, int width,
+                               int height, int band, int paths, int disparities, float uniqueness,
+                               float *disparity, uint32_t *keys, cudaStream_t stream);
+int band_lane_values(int band);
+
+// The band matcher's scratch: both images' codes, the bases (when the
+// search makes them), the band costs and path volumes, selection's outputs.
+struct BandScratch {
+    uint64_t *left_codes, *right_codes;
+    int32_t *base;
+    uint8_t *costs, *paths;
+    float *selected;
+    uint32_t *keys;
+};
+size_t band_scratch_bytes(int width, int height, int band);
+BandScratch carve_band_scratch(void *base, int width, int height, int band);
+// band_scratch_bytes plus the half images, the coarse disparity and the
+// coarse matcher's scratch.
+size_t coarse_to_fine_scratch_bytes(int width, int height, int band);
+
+// sgm_band/4 on device buffers: `base` s32 [height][width].
+cudaError_t run_band_matcher(const uint8_t *left, const uint8_t *right, const int32_t *base,
+                             int width, int height, int disparities, int paths, int band,
+                             int window, int p1, int p2, float uniqueness, int stage_mask,
+                             const BandScratch &scratch, float *disparity, cudaStream_t stream);
+// sgm_coarse_to_fine/3 on device buffers (even width and height); the bases
+// go to base_out when it is not null. `scratch` holds
+// coarse_to_fine_scratch_bytes.
+cudaError_t run_coarse_to_fine(const uint8_t *left, const uint8_t *right, int width, int height,
+                               int paths, int coarse_paths, int band, int margin, int window,
+                               int p1, int p2, float uniqueness, int stage_mask, void *scratch,
+                               float *disparity, int32_t *base_out, cudaStream_t stream);
+
 // The device a context was opened on.
 int context_device(nxs_context *context);
 

@@ -67,6 +67,14 @@ class SgmParams(ctypes.Structure):
                 ("uniqueness", ctypes.c_float), ("stage_mask", ctypes.c_uint32)]
 
 
+class BandParams(ctypes.Structure):
+    _fields_ = [("sgm", SgmParams), ("band", ctypes.c_uint32), ("margin", ctypes.c_uint32),
+                ("coarse_paths", ctypes.c_uint32), ("census", ctypes.c_uint32)]
+
+
+CENSUS_WINDOWS = {"sparse_9x7": 0, "dense_9x5": 1, "dense_9x5_blend": 2}
+
+
 class Camera(ctypes.Structure):
     _fields_ = [("k", ctypes.c_float * 9), ("d", ctypes.c_float * 5),
                 ("inverse_pr", ctypes.c_float * 9)]
@@ -119,6 +127,14 @@ SIGNATURES = {
     "nxs_sgm_scratch_bytes": (_u64, [_u32, _u32, _u32]),
     "nxs_set_path_words": (_i, [_u32, _u32]),
     "nxs_path_words": (_u32, [_u32]),
+    "nxs_band_check": (_i, [ctypes.POINTER(BandParams), _u32, _u32, ctypes.c_int32] + _err),
+    "nxs_band_scratch_bytes": (_u64, [_u32, _u32, _u32, ctypes.c_int32]),
+    "nxs_sgm_band_device": (_i, [_P, _P, _P, _P, _u32, _u32, ctypes.POINTER(BandParams), _P, _P]
+                            + _err),
+    "nxs_sgm_coarse_to_fine_device": (_i, [_P, _P, _P, _u32, _u32, ctypes.POINTER(BandParams),
+                                           _P, _P, _P] + _err),
+    "nxs_sgm_coarse_to_fine": (_i, [_P, _P, _P, _u32, _u32, ctypes.POINTER(BandParams), _P]
+                               + _err),
     "nxs_census_device": (_i, [_P, _u32, _u32, _P, _P]),
     "nxs_census_pair_device": (_i, [_P, _P, _u32, _u32, _P, _P, _P]),
     "nxs_check_median_device": (_i, [_P, _P, _u32, _u32, _u32, _P, _P]),
@@ -198,6 +214,21 @@ def _errbuf():
 def sgm_params(disparities=64, paths=8, p1=8, p2=64, uniqueness=1.0526315789473684,
                stage_mask=False):
     return SgmParams(disparities, paths, p1, p2, uniqueness, 1 if stage_mask else 0)
+
+
+def band_params(disparities=128, paths=8, p1=8, p2=64, uniqueness=1.0526315789473684,
+                stage_mask=False, band=16, margin=4, coarse_paths=None, census="sparse_9x7"):
+    return BandParams(sgm_params(disparities, paths, p1, p2, uniqueness, stage_mask), band,
+                      margin, coarse_paths or paths, CENSUS_WINDOWS[census])
+
+
+def check_band(width, height, coarse_to_fine=True, **settings):
+    """(True, "") or (False, why) for sgm_coarse_to_fine/3 (or sgm_band/4)."""
+    p = band_params(**settings)
+    buf = _errbuf()
+    status = load().nxs_band_check(ctypes.byref(p), width, height, 1 if coarse_to_fine else 0,
+                                   buf, 1024)
+    return (status == OK, buf.value.decode() if status != OK else "")
 
 
 def check_sgm(width, height, **settings):
@@ -397,11 +428,43 @@ class Context:
                               ctypes.byref(p), out.ctypes.data, buf, 1024), buf)
         return out
 
+    def sgm_coarse_to_fine(self, left, right, **settings):
+        """NxStereo.sgm_coarse_to_fine/3 on a host pair (band_params' settings)."""
+        left = np.ascontiguousarray(left, np.uint8)
+        right = np.ascontiguousarray(right, np.uint8)
+        h, w = left.shape
+        out = np.empty((h, w), np.float32)
+        p = band_params(**settings)
+        buf = _errbuf()
+        _check(load().nxs_sgm_coarse_to_fine(self._handle, left.ctypes.data, right.ctypes.data,
+                                             w, h, ctypes.byref(p), out.ctypes.data, buf, 1024),
+               buf)
+        return out
+
+    def sgm_coarse_to_fine_device(self, d_left, d_right, width, height, d_out, d_base=None,
+                                  stream=0, **settings):
+        p = band_params(**settings)
+        buf = _errbuf()
+        _check(load().nxs_sgm_coarse_to_fine_device(self._handle, d_left, d_right, width, height,
+                                                    ctypes.byref(p), d_out, d_base, stream, buf,
+                                                    1024), buf)
+
+    def sgm_band_device(self, d_left, d_right, d_base, width, height, d_out, stream=0,
+                        **settings):
+        p = band_params(**settings)
+        buf = _errbuf()
+        _check(load().nxs_sgm_band_device(self._handle, d_left, d_right, d_base, width, height,
+                                          ctypes.byref(p), d_out, stream, buf, 1024), buf)
+
     def sgm_device(self, d_left, d_right, width, height, d_out, stream=0, **settings):
         p = sgm_params(**settings)
         buf = _errbuf()
         _check(load().nxs_sgm_device(self._handle, d_left, d_right, width, height,
                                      ctypes.byref(p), d_out, stream, buf, 1024), buf)
+
+
+def band_scratch_bytes(width, height, band, coarse_to_fine=True):
+    return int(load().nxs_band_scratch_bytes(width, height, band, 1 if coarse_to_fine else 0))
 
 
 def scratch_bytes(width, height, disparities):

@@ -11,7 +11,8 @@ Settings, defaults, ranges and refusals are the reference's
 (stage/disparity.ex:35-114, stage/rectification.ex:28-45,
 stage/speckle_filter.ex:13-47, stage/temporal_filter.ex:25-59,
 stage/depth.ex:19-22, stage/point_cloud.ex:58-121, stage/quality.ex:12-24).
-Beyond the reference, Disparity also takes num_disparities of 96, 192 and 256.
+Beyond the reference, Disparity also takes num_disparities of 96, 192 and 256,
+and its coarse-to-fine search may be pinned to the native matcher.
 """
 import numpy as np
 
@@ -174,7 +175,17 @@ class Disparity(Stage):
             ("num_disparities", {"default": 64, "type": "integer",
                                  "values": [64, 96, 128, 192, 256]}),
             ("paths", {"default": 8, "type": "integer", "values": [3, 8]}),
-            ("search", {"default": "full", "type": "string", "values": ["full"]}),
+            ("search", {"default": "full", "type": "string",
+                        "values": ["full", "coarse_to_fine"]}),
+            ("coarse_paths", {"when": {"search": "coarse_to_fine"}, "default": None,
+                              "type": "integer", "values": [3, 8]}),
+            ("band", {"when": {"search": "coarse_to_fine"}, "default": 16, "type": "integer",
+                      "values": [8, 16, 32, 64]}),
+            ("margin", {"when": {"search": "coarse_to_fine"}, "default": 4, "type": "integer",
+                        "range": (0, 63)}),
+            ("fine_census", {"when": {"search": "coarse_to_fine"}, "default": "sparse_9x7",
+                             "type": "atom",
+                             "values": ["sparse_9x7", "dense_9x5", "dense_9x5_blend"]}),
             ("matcher", {"default": None, "type": "atom", "values": [None, "nx", "native"]}),
         ]
 
@@ -188,7 +199,28 @@ class Disparity(Stage):
 
     @staticmethod
     def init(given, geometry):
-        return init_settings(Disparity, given)
+        """stage/disparity.ex:120-128 and its checks (196-219). Beyond the
+        reference, the coarse-to-fine search may be pinned to the native
+        matcher (matcher "native"): this library computes it."""
+        status, state = init_settings(Disparity, given)
+        if status != "ok":
+            return (status, state)
+        if state["coarse_paths"] is None:
+            state["coarse_paths"] = state["paths"]
+        if state["search"] == "coarse_to_fine":
+            if state["num_disparities"] != 128:
+                return ("error", "coarse_to_fine searches 128 disparities, got "
+                                 f"{state['num_disparities']}")
+            width, height = geometry["width"], geometry["height"]
+            if width % 2 or height % 2:
+                return ("error", f"coarse_to_fine needs an even width and height, got "
+                                 f"{width}x{height}")
+            if state["margin"] >= state["band"]:
+                return ("error", f"margin must be below band ({state['band']}), got "
+                                 f"{state['margin']}")
+        elif state["fine_census"] != "sparse_9x7":
+            return ("error", "fine_census requires coarse_to_fine search")
+        return ("ok", state)
 
     @staticmethod
     def params(state, geometry):
@@ -196,7 +228,10 @@ class Disparity(Stage):
 
     @staticmethod
     def compute(state):
-        return state["matcher"]
+        """stage/disparity.ex:165-166: coarse_to_fine is computed in Nx unless pinned."""
+        if state.get("search") == "coarse_to_fine":
+            return state.get("matcher") or "nx"
+        return state.get("matcher")
 
     @staticmethod
     def native_kind():
@@ -204,7 +239,15 @@ class Disparity(Stage):
 
     @staticmethod
     def native_settings(state):
-        return [("num_disparities", state["num_disparities"]), ("paths", state["paths"])]
+        """The member's build settings (stage/disparity.ex:171); the
+        coarse-to-fine search adds its own, the census window as its index."""
+        out = [("num_disparities", state["num_disparities"]), ("paths", state["paths"])]
+        if state["search"] == "coarse_to_fine":
+            windows = ["sparse_9x7", "dense_9x5", "dense_9x5_blend"]
+            out += [("coarse_to_fine", 1), ("band", state["band"]), ("margin", state["margin"]),
+                    ("coarse_paths", state["coarse_paths"]),
+                    ("fine_census", windows.index(state["fine_census"]))]
+        return out
 
 
 class SpeckleFilter(Stage):

@@ -261,3 +261,58 @@ def test_camera_mirrors_rectify_camera():
     moved = rectify.move_rows(cam, 2.0)
     assert moved["inverse_pr"][1, 2] == np.float32(cam["inverse_pr"][1, 2] +
                                                    np.float32(2.0) * cam["inverse_pr"][1, 1])
+
+
+def test_band_check_refuses_what_the_coarse_to_fine_search_refuses():
+    # sgm_band/4 (lib/nx_stereo.ex:300-304) and sgm_coarse_to_fine/3 (173-183)
+    assert native.check_band(64, 48) == (True, "")
+    assert native.check_band(65, 48, coarse_to_fine=False, disparities=64) == (True, "")
+    refusals = [((65, 48), {}, "even height and width"),
+                ((64, 48), dict(disparities=64), "must be 128"),
+                ((64, 48), dict(band=12), ":band must be 8, 16, 32 or 64"),
+                ((64, 48), dict(census="dense_9x5", coarse_paths=4), "coarse_paths"),
+                ((64, 48), dict(margin=128), "margin"),
+                ((16, 48), {}, "wider than 8"),  # the half-size pair is 8 wide
+                ((64, 12), {}, "higher than 6")]
+    for (w, h), settings, why in refusals:
+        ok, message = native.check_band(w, h, **settings)
+        assert not ok and why in message, (w, h, settings, message)
+    ok, message = native.check_band(64, 48, coarse_to_fine=False, band=12)
+    assert not ok and ":band" in message
+    p = native.band_params()
+    p.census = 3
+    buf = native._errbuf()
+    assert native.load().nxs_band_check(ctypes.byref(p), 64, 48, 1, buf, 1024) == \
+        native.BAD_ARGUMENT
+    assert native.band_scratch_bytes(728, 544, 16) > native.band_scratch_bytes(728, 544, 16, False)
+
+
+def test_coarse_to_fine_settings_and_refusals():
+    # stage/disparity.ex:72-108, 120-128, 165-166, 196-219
+    geometry = {**GEOMETRY, "width": 64, "height": 48}
+    status, state = stage.Disparity.init({"search": "coarse_to_fine", "num_disparities": 128},
+                                         geometry)
+    assert status == "ok"
+    assert (state["band"], state["margin"], state["coarse_paths"], state["fine_census"]) == \
+        (16, 4, 8, "sparse_9x7")
+    assert stage.Disparity.compute(state) == "nx"  # computed in Nx unless pinned
+    assert not segment.CudaSegment.accepts(stage.Disparity, state, "native")
+    status, native_state = stage.Disparity.init(
+        {"search": "coarse_to_fine", "num_disparities": 128, "matcher": "native", "band": 32,
+         "coarse_paths": 3, "fine_census": "dense_9x5_blend"}, geometry)
+    assert status == "ok" and stage.Disparity.compute(native_state) == "native"
+    assert segment.CudaSegment.accepts(stage.Disparity, native_state, "native")
+    assert stage.Disparity.native_settings(native_state) == [
+        ("num_disparities", 128), ("paths", 8), ("coarse_to_fine", 1), ("band", 32),
+        ("margin", 4), ("coarse_paths", 3), ("fine_census", 2)]
+    refusals = [({"search": "coarse_to_fine"}, geometry, "searches 128 disparities, got 64"),
+                ({"search": "coarse_to_fine", "num_disparities": 128}, {**geometry, "width": 63},
+                 "even width and height, got 63x48"),
+                ({"search": "coarse_to_fine", "num_disparities": 128, "band": 8, "margin": 8},
+                 geometry, "margin must be below band (8), got 8"),
+                ({"fine_census": "dense_9x5"}, geometry, "fine_census requires coarse_to_fine"),
+                ({"search": "coarse_to_fine", "num_disparities": 128, "band": 12}, geometry,
+                 "band must be one of")]
+    for given, g, why in refusals:
+        status, message = stage.Disparity.init(given, g)
+        assert status == "error" and why in message, (given, message)
