@@ -14,8 +14,10 @@ image), timed as the max over ranks.
 Beside the headline, rank 0 of a one-GPU run also reports `batched` (64
 rectified pairs of mixed sizes and disparity ranges in one persistent,
 graph-captured launch, against the single-pair matcher on the same pairs),
-`large_range` (8 pairs of 1920x1080 at 256 disparities) and `serving` (32
-camera streams with Poisson arrivals at 30 pairs/s each: p50/p99 latency).
+`large_range` (8 pairs of 1920x1080 at 256 disparities), `coarse_to_fine`
+(Stage.Disparity's coarse-to-fine search at 728x544, band 16, beside the full
+search) and `serving` (32 camera streams with Poisson arrivals at 30 pairs/s
+each: p50/p99 latency).
 
 `--impl reference` times the reference's CPU formulation of the same pipeline
 (the oracle's C port of the reference's Rust matcher and stages) on all host
@@ -50,6 +52,14 @@ SERVING_CAP = None
 PATHS_TRAFFIC_BYTES = 107_285_504 + 350_222_336
 
 
+# The workload's config, the same on both arms.
+CONFIG = {"workload": "full pipeline 728x544 frames -> 728x544, D128, 8 paths, despeckle, depth, "
+                      "cloud (decimation 4)",
+          "width": WIDTH, "height": HEIGHT, "disparities": DISPARITIES, "paths": PATHS,
+          "decimation": DECIMATION, "pairs_per_step": 1}
+E2E_MIN_SECONDS = 1.0  # the end-to-end loop runs at least this long (and at least --steps pairs)
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -61,6 +71,8 @@ def parse():
     p.add_argument("--no-batch", action="store_true", help="skip the batched workload")
     p.add_argument("--no-serving", action="store_true", help="skip the serving workload")
     p.add_argument("--no-large", action="store_true", help="skip the large-range workload")
+    p.add_argument("--no-coarse-to-fine", action="store_true",
+                   help="skip the coarse-to-fine workload")
     return p.parse_args()
 
 
@@ -270,9 +282,6 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         stage_ms = {name: statistics.mean(m[k].elapsed_time(m[k + 1]) for m in stage_marks)
                     for k, name in enumerate(DevicePipeline.STAGES)}
-    # The clock record covers the device-timed steps; the sampler's reader
-    # thread stops before the host-bound end-to-end loop.
-    sampler.stop()
     total_s = replicas.max_over_ranks(sum(step_ms) / 1000.0, device="cuda")
     value = replicas.whole_job_rate(args.steps, world, total_s)
 
@@ -311,18 +320,30 @@ def run_ours(args, rank, world, local_rank):
     replicas.barrier()
     # The cyclic collector paused for the timed loop, as the serving loop does:
     # a collection of the replies' objects stalls the host for milliseconds.
+    # The loop sends --steps pairs at a time until it has run E2E_MIN_SECONDS;
+    # every rank runs the same number of rounds (the first rank's count).
     collecting = gc.isenabled()
     gc.disable()
     try:
         e0 = time.perf_counter()
-        e2e_loop(args.steps)
-        torch.cuda.synchronize()
+        e2e_pairs = 0
+        while True:
+            e2e_loop(args.steps)
+            e2e_pairs += args.steps
+            torch.cuda.synchronize()
+            more = time.perf_counter() - e0 < E2E_MIN_SECONDS
+            if not replicas.agree(more, device="cuda"):
+                break
         e_elapsed = time.perf_counter() - e0
+        e1 = time.monotonic()
     finally:
         if collecting:
             gc.enable()
     e_s = replicas.max_over_ranks(e_elapsed, device="cuda")
-    clocks = sampler.summary(t0, t1)
+    sampler.stop()
+    # Device-timed steps are short (milliseconds), so the clock record spans
+    # them, the stage-time run and the end-to-end loop: all under load.
+    clocks = sampler.summary(t0, e1)
     seg.release()
 
     peak, peak_kind = peaks()
@@ -337,12 +358,9 @@ def run_ours(args, rank, world, local_rank):
         "ms_per_step": round(statistics.mean(step_ms), 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/u16",
         "data": "synthetic (seeded piecewise-planar scenes, raw frames from a synthetic rig)",
-        "config": {"workload": "full pipeline 728x544 frames -> 728x544, D128, 8 paths, "
-                               "despeckle, depth, cloud (decimation 4)",
-                   "width": WIDTH, "height": HEIGHT, "disparities": DISPARITIES, "paths": PATHS,
-                   "pairs_per_step": 1, "parallelism": f"replicas x{world}",
-                   "l2": "flushed between steps (256 MiB write outside the step events); "
-                         "per-step working set 460 MB > 126 MB L2"},
+        "config": dict(CONFIG, parallelism=f"replicas x{world}",
+                       l2="flushed between steps (256 MiB write outside the step events); "
+                          "per-step working set 460 MB > 126 MB L2"),
         "mdisp_s": round(value * px * DISPARITIES / 1e6, 1),
         "gpu_launches": KERNELS_PER_STEP * args.steps,
         "roofline": {"bound": "hbm", "kernel": "paths_kernel (8-path aggregation)",
@@ -358,9 +376,10 @@ def run_ours(args, rank, world, local_rank):
         "pipeline_roofline": {"b_alg_per_pair": b_alg,
                               "achieved_gbs": round(b_alg * value / world / 1e9, 1),
                               "frac": round(b_alg * value / world / 1e9 / peak, 4)},
-        "e2e": {"value": round(replicas.whole_job_rate(args.steps, world, e_s), 2),
+        "e2e": {"value": round(replicas.whole_job_rate(e2e_pairs, world, e_s), 2),
                 "unit": "pairs/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "pairs": e2e_pairs, "seconds": round(e_s, 3),
                 "api": "CudaSegment.send_request/await_ (C ABI nxs_run_async), depth "
                        f"{mod.depth()}, cyclic garbage collector paused while timed"},
         "clocks": clocks,
@@ -406,13 +425,7 @@ def _plain_and_batched(torch, ctx, shapes, pairs, tuner_search=None, repeats=5):
     for _ in range(3):
         plan.run(copy=False)
     e2e_s = (time.perf_counter() - t0) / 3
-    # The plain form end to end: nxs_sgm on each pair's host images in turn.
-    for (w, h, settings), (left, right) in zip(shapes[:2], pairs[:2]):
-        ctx.sgm(left, right, **settings)
-    t0 = time.perf_counter()
-    for (w, h, settings), (left, right) in zip(shapes, pairs):
-        ctx.sgm(left, right, **settings)
-    plain_e2e_s = time.perf_counter() - t0
+    plain_e2e_s, pipelined_exact = _plain_pipelined(shapes, pairs, host_outputs)
     devs = [(torch.from_numpy(l).cuda(), torch.from_numpy(r).cuda()) for l, r in pairs]
     outs = [torch.empty((h, w), dtype=torch.float32, device="cuda") for w, h, _ in shapes]
 
@@ -440,12 +453,79 @@ def _plain_and_batched(torch, ctx, shapes, pairs, tuner_search=None, repeats=5):
             "e2e_pairs_per_s": round(n / e2e_s, 1),
             "plain_e2e_pairs_per_s": round(n / plain_e2e_s, 1),
             "batched_over_plain_e2e": round(plain_e2e_s / e2e_s, 3),
-            "plain_e2e_api": "nxs_sgm per pair (host images in, disparity out, synchronous)",
+            "plain_e2e_api": "the pipelined per-pair API: a CudaSegment (Stage.Disparity) per "
+                             "distinct shape, pinned staging, pairs sent in order with up to "
+                             f"{PIPELINE_DEPTH} at the device (C ABI nxs_run_async)",
+            "plain_e2e_exact_pairs": pipelined_exact,
             "e2e_api": "BatchPlan.run (C ABI nxs_batch_run: one graph, host in and out)",
             "h2d_bytes": stats["input_bytes"], "d2h_bytes": stats["output_bytes"],
             "bit_exact_pairs": exact, "tuning": tuning, "queue_items": stats["items"],
             "device_gb": round(stats["device_bytes"] / 1e9, 2),
             "b_alg_gbs": round(b_alg / batched_ms / 1e6, 1), "gpu_launches_per_batch": 1}
+
+
+PIPELINE_DEPTH = 4
+
+
+def _plain_pipelined(shapes, pairs, batch_outputs, depth=PIPELINE_DEPTH):
+    """The single-pair form end to end through the public per-pair API: a
+    CudaSegment with Stage.Disparity alone for each distinct shape (pinned
+    staging, two compute lanes), the pairs sent in order with up to `depth`
+    at the device. Returns (seconds, pairs equal to the batch's outputs
+    after Stage.Disparity's mask)."""
+    from nx_stereo_b200 import segment, stage
+
+    mod = segment.CudaSegment
+    segments = {}
+
+    def segment_of(w, h, settings):
+        key = (w, h, settings["disparities"], settings.get("paths", 8))
+        if key not in segments:
+            geometry = segment.standard_geometry(w, h)
+            status, members = segment.members(
+                [(stage.Disparity, {"num_disparities": key[2], "paths": key[3]})], geometry)
+            assert status == "ok", members
+            status, segments[key] = mod.build(members, geometry)
+            assert status == "ok", segments[key]
+        return segments[key]
+
+    def loop():
+        inflight, outputs = [], []
+
+        def reply():
+            request, seg = inflight.pop(0)
+            answer = mod.await_(request, seg, 60000)
+            assert answer[0] == "ok", answer
+            outputs.append(np.array(answer[1]["disparity"]))
+
+        for (w, h, settings), (left, right) in zip(shapes, pairs):
+            seg = segment_of(w, h, settings)
+            status, request = mod.send_request({"left": left, "right": right}, seg)
+            assert status == "ok", request
+            inflight.append((request, seg))
+            if len(inflight) >= depth:
+                reply()
+        while inflight:
+            reply()
+        return outputs
+
+    loop()  # configures every segment (device memory, pinned staging)
+    collecting = gc.isenabled()
+    gc.disable()
+    try:
+        t0 = time.perf_counter()
+        outputs = loop()
+        seconds = time.perf_counter() - t0
+    finally:
+        if collecting:
+            gc.enable()
+    exact = sum(int(np.array_equal(o.view(np.uint32),
+                                   np.where(b > 0, b, np.float32(-1.0)).astype(np.float32)
+                                   .view(np.uint32)))
+                for o, b in zip(outputs, batch_outputs))
+    for seg in segments.values():
+        seg.release()
+    return seconds, exact
 
 
 def bench_batched(torch, ctx):
@@ -473,7 +553,129 @@ def bench_large(torch, ctx):
                              tuner_search={"engine": (0, 1), "streams": (1, 2, 8),
                                            "order": (0, 1), "group_pairs": (1, 2)})
     out["workload"] = "8 pairs 1920x1080, 256 disparities, 8 paths"
+    out.update(_large_overlap(torch, ctx, shapes, pairs))
     return out
+
+
+def _large_overlap(torch, ctx, shapes, pairs):
+    """The large-range batch with each pair's kernels as a chain on 1, 2 or 4
+    streams of one graph (with 2, pair k + 1's census and costs run beside
+    pair k's path aggregation) and as the persistent launch, each timed by
+    CUDA events; and one pair's stages, each bracketed by events."""
+    from nx_stereo_b200 import batch, native
+
+    stream = torch.cuda.Stream()
+    handle = stream.cuda_stream
+    plan = batch.BatchPlan(ctx, shapes, {"engine": 1, "streams": 1})
+    for i, (left, right) in enumerate(pairs):
+        plan.set_inputs(i, left, right)
+    want = plan.run()
+    streams_ms = {}
+    for count in (1, 2, 4):
+        plan.retune(engine=1, streams=count)
+        with torch.cuda.stream(stream):
+            plan.launch(stream=handle)
+        streams_ms[str(count)] = round(
+            _time_events(torch, stream, lambda: plan.launch(stream=handle), 3), 3)
+    plan.retune(engine=0)
+    with torch.cuda.stream(stream):
+        plan.launch(stream=handle)
+    persistent_ms = round(_time_events(torch, stream, lambda: plan.launch(stream=handle), 3), 3)
+    got = plan.run()
+    exact = sum(int(np.array_equal(a.view(np.uint32), b.view(np.uint32))) for a, b in zip(got, want))
+    plan.close()
+    # One pair's stages on device buffers, in the order the matcher runs them.
+    w, h, d = 1920, 1080, 256
+    span = int(native.load().nxs_matcher_span(d))
+    dl, dr = (torch.from_numpy(a).cuda() for a in pairs[0])
+    costs = torch.empty(w * h * d, dtype=torch.uint8, device="cuda")
+    volumes = torch.empty(8 * w * h * d, dtype=torch.uint8, device="cuda")
+    selected = torch.empty(w * h, dtype=torch.float32, device="cuda")
+    keys = torch.empty(w * h, dtype=torch.int32, device="cuda")
+    out = torch.empty(w * h, dtype=torch.float32, device="cuda")
+    steps = {
+        "census_costs": lambda: native.call("nxs_census_costs_device_ordered", dl.data_ptr(),
+                                            dr.data_ptr(), w, h, d, span, costs.data_ptr(),
+                                            handle),
+        "paths": lambda: native.call("nxs_paths_device_ordered", costs.data_ptr(), w, h, d, 8, 8,
+                                     64, span, volumes.data_ptr(), handle),
+        "select": lambda: native.call("nxs_select_paths_device_ordered", volumes.data_ptr(), w, h,
+                                      d, 8, 1.0526315789473684, span, selected.data_ptr(),
+                                      keys.data_ptr(), handle),
+        "check_median": lambda: native.call("nxs_check_median_device", selected.data_ptr(),
+                                            keys.data_ptr(), w, h, 0, out.data_ptr(), handle),
+    }
+    stage_ms = {}
+    for name, fn in steps.items():
+        with torch.cuda.stream(stream):
+            fn()
+        stage_ms[name] = round(_time_events(torch, stream, fn, 3), 3)
+    del costs, volumes
+    return {"streams_engine_ms": streams_ms, "persistent_ms": persistent_ms,
+            "overlap_exact_pairs": exact, "pair_stages_ms": stage_ms,
+            "overlap_note": "streams_engine_ms: each pair's kernels chained on one of k streams "
+                            "of one CUDA graph, so with k >= 2 the next pair's census and "
+                            "costs run beside the current pair's path aggregation"}
+
+
+def bench_coarse_to_fine(torch, ctx, pairs=64):
+    """Stage.Disparity's coarse-to-fine search at 728x544 (band 16, margin 4,
+    8 paths, the reference's fast setting): CUDA-event ms a pair on device
+    buffers, beside the full search of the same rectified pairs; both checked
+    against the oracle on the first pair."""
+    from nx_stereo_b200 import scene
+    from oracle import oracle
+
+    w, h = WIDTH, HEIGHT
+    inputs = [scene.rectified_pair(w, h, seed=3000 + i, rectangles=6, max_disparity=120)
+              for i in range(8)]
+    devs = [(torch.from_numpy(l).cuda(), torch.from_numpy(r).cuda()) for l, r in inputs]
+    out = torch.empty((h, w), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    handle = stream.cuda_stream
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    settings = {"band": 16, "margin": 4, "paths": PATHS}
+
+    def c2f(i):
+        dl, dr = devs[i % len(devs)]
+        ctx.sgm_coarse_to_fine_device(dl.data_ptr(), dr.data_ptr(), w, h, out.data_ptr(),
+                                      stream=handle, **settings)
+
+    def full(i):
+        dl, dr = devs[i % len(devs)]
+        ctx.sgm_device(dl.data_ptr(), dr.data_ptr(), w, h, out.data_ptr(), stream=handle,
+                       disparities=DISPARITIES, paths=PATHS)
+
+    results = {}
+    for name, fn in (("coarse_to_fine", c2f), ("full", full)):
+        marks = []
+        with torch.cuda.stream(stream):
+            for i in range(3):
+                fn(i)
+            for i in range(pairs):
+                flush.fill_(i & 0xFF)
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                fn(i)
+                b.record(stream)
+                marks.append((a, b))
+        torch.cuda.synchronize()
+        results[name] = statistics.mean(a.elapsed_time(b) for a, b in marks)
+    left, right = inputs[0]
+    c2f(0)
+    torch.cuda.synchronize()
+    want = oracle.sgm_coarse_to_fine(left, right, PATHS, PATHS, 16, 4)
+    exact = bool(np.array_equal(out.cpu().numpy().view(np.uint32), want.view(np.uint32)))
+    return {"workload": "728x544 rectified pairs, coarse to fine: sgm/3 at 364x272 D64 8 paths, "
+                        "then sgm_band/4 D128 band 16 margin 4 8 paths (+ check, median)",
+            "pairs": pairs, "ms_per_pair": round(results["coarse_to_fine"], 4),
+            "pairs_per_s": round(1000.0 / results["coarse_to_fine"], 1),
+            "full_search_ms_per_pair": round(results["full"], 4),
+            "over_full_search": round(results["full"] / results["coarse_to_fine"], 3),
+            "bit_exact_first_pair": exact,
+            "timing": "CUDA events around each pair on device buffers, L2 flushed between "
+                      "pairs outside the events"}
 
 
 def bench_serving(seconds=3.0, max_in_flight=SERVING_CAP):
@@ -558,8 +760,7 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * threads / value, 2),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/u16",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": "full pipeline 728x544 frames -> 728x544, D128, 8 paths, "
-                                   "despeckle, depth, cloud (decimation 4)"},
+            "config": dict(CONFIG, parallelism=f"{threads} host threads"),
             "cpu_baseline": {"value": round(value, 3), "unit": "pairs/s", "cores": threads,
                              "kind": "port", "sample": sample},
             "e2e": {"value": round(value, 3), "unit": "pairs/s", "h2d_bytes_per_step": 0,
@@ -592,6 +793,8 @@ def main():
             line["batched"] = bench_batched(torch, ctx)
         if not args.no_large:
             line["large_range"] = bench_large(torch, ctx)
+        if not args.no_coarse_to_fine:
+            line["coarse_to_fine"] = bench_coarse_to_fine(torch, ctx)
         ctx.close()
         if not args.no_serving:
             line["serving"] = bench_serving()

@@ -16,15 +16,16 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBRARY = os.path.join(HERE, "libnxs_b200.so")
+PORT = os.path.join(HERE, "nxs_port")
 SOURCES = ["matcher.cu", "stages.cu", "abi.cu", "matcher_static.cu", "batch.cu", "band.cu"]
-HEADERS = ["nxs_device.cuh", "nxs_kernels.h", "nxs_matcher.cuh"]
+HEADERS = ["nxs_device.cuh", "nxs_kernels.h", "nxs_matcher.cuh", "port_records.h", "port.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-fmad=false", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr"]
 
 
 def _stale():
-    if not os.path.exists(LIBRARY):
+    if not os.path.exists(LIBRARY) or not os.path.exists(PORT):
         return True
     inputs = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
     inputs.append(os.path.join(ROOT, "include", "nx_stereo_b200.h"))
@@ -53,6 +54,10 @@ def build(force=False, verbose=False):
     subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp]
                    + objects + ["-lcudart_static", "-lrt", "-ldl", "-lpthread"], check=True)
     os.replace(tmp, LIBRARY)
+    # nxs_port: the stereo_match Port protocol over the library (found beside it).
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", PORT + ".tmp", os.path.join(CSRC, "port.cpp"),
+                    "-L", HERE, "-lnxs_b200", "-Wl,-rpath,$ORIGIN", "-lpthread"], check=True)
+    os.replace(PORT + ".tmp", PORT)
     return LIBRARY
 
 

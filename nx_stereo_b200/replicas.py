@@ -40,6 +40,19 @@ def max_over_ranks(value, device="cpu"):
     return float(t.item())
 
 
+def agree(flag, device="cpu"):
+    """Rank 0's `flag` on every rank (the flag itself with one rank), so that
+    every rank takes the same number of rounds of a loop with collectives."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return bool(flag)
+    t = torch.tensor([1 if flag else 0], dtype=torch.int32, device=device)
+    dist.broadcast(t, src=0)
+    return bool(t.item())
+
+
 def barrier():
     import torch.distributed as dist
 

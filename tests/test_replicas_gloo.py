@@ -30,9 +30,16 @@ def _rank(rank, world_size, port, out_dir):
     seconds = 0.5 + 0.25 * rank  # the ranks' timed regions, as they measured them
     slowest = replicas.max_over_ranks(seconds)
     rate = replicas.whole_job_rate(10, world_size, slowest)
+    # A loop whose length rank 0 decides (the end-to-end loop's rounds): every
+    # rank takes as many rounds as rank 0, whatever its own flag says.
+    rounds = 0
+    while True:
+        rounds += 1
+        if not replicas.agree(rounds < 3 if rank == 0 else rounds < 10):
+            break
     np.save(os.path.join(out_dir, f"rank{rank}.npy"), disparity)
     with open(os.path.join(out_dir, f"rank{rank}.txt"), "w") as f:
-        f.write(f"{slowest} {rate}")
+        f.write(f"{slowest} {rate} {rounds}")
     replicas.barrier()
     import torch.distributed as dist
 
@@ -44,8 +51,9 @@ def test_two_gloo_ranks_run_independent_replicas_and_reduce_only_time(tmp_path, 
 
     mp.spawn(_rank, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True)
     results = [open(tmp_path / f"rank{r}.txt").read().split() for r in range(2)]
-    assert all(float(slowest) == 0.75 for slowest, _ in results)
-    assert all(float(rate) == pytest.approx(20 / 0.75) for _, rate in results)
+    assert all(float(slowest) == 0.75 for slowest, _, _ in results)
+    assert all(float(rate) == pytest.approx(20 / 0.75) for _, rate, _ in results)
+    assert [int(rounds) for _, _, rounds in results] == [3, 3]
     from nx_stereo_b200 import replicas
 
     outputs = [np.load(tmp_path / f"rank{r}.npy") for r in range(2)]
