@@ -200,6 +200,16 @@ nxs_status nxs_sgm_check(const nxs_sgm_params *params, uint32_t width, uint32_t 
 nxs_status nxs_set_path_words(uint32_t disparities, uint32_t words);
 uint32_t nxs_path_words(uint32_t disparities);
 
+/* How the matcher aggregates the 8 (or 3) directions before selection
+ * (lib/nx_stereo.ex:545-573, one sum per pixel and disparity): mode 0 (the
+ * default) keeps each direction's u8 path volume and selection sums them;
+ * mode 1 has every direction add its path costs into one u16 aggregate
+ * volume in L2 as it scans (nxs_path_sums_device), which measured slower. A
+ * tuning knob for the whole library; results do not depend on it.
+ * nxs_path_sums: 1 where the matcher sums at that size. */
+nxs_status nxs_set_path_sums(uint32_t mode);
+uint32_t nxs_path_sums(uint32_t width, uint32_t height, uint32_t disparities);
+
 /* The disparity of each left pixel, -1.0 where unmatched: NxStereo.sgm/3 on a
  * rectified u8 pair in host memory (lib/nx_stereo.ex:64-74; natively
  * Matcher::disparity, native/stereo_match/src/lib.rs:105-124). Synchronous. */
@@ -350,6 +360,20 @@ nxs_status nxs_select_paths_device_ordered(const uint8_t *d_paths, uint32_t widt
                                            uint32_t height, uint32_t disparities, uint32_t paths,
                                            float uniqueness, uint32_t span, float *d_disparity,
                                            uint32_t *d_keys, void *stream);
+
+/* The aggregation as one sum (lib/nx_stereo.ex:545-573, the sum of the
+ * direction volumes that selection reads): every direction's path costs from
+ * costs in the span-16 order added, as the scan goes, into d_sums, a u16
+ * volume of width x height x disparities values (disparities a multiple of
+ * 16, 64..256) that the call zeroes first and keeps in its own layout; then
+ * selection over it, as nxs_select_paths_device_ordered over the path
+ * volumes. The two give the same disparities and keys. */
+nxs_status nxs_path_sums_device(const uint8_t *d_costs, uint32_t width, uint32_t height,
+                                uint32_t disparities, uint32_t paths, uint32_t p1, uint32_t p2,
+                                uint16_t *d_sums, void *stream);
+nxs_status nxs_select_path_sums_device(const uint16_t *d_sums, uint32_t width, uint32_t height,
+                                       uint32_t disparities, float uniqueness,
+                                       float *d_disparity, uint32_t *d_keys, void *stream);
 
 /* Winner, uniqueness and subpixel from u16 sums: f32 disparity and u32 keys
  * (lib/nx_stereo.ex:608-641). */

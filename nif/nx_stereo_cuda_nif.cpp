@@ -22,7 +22,7 @@
 // process exits (matcher.ex:148-160).
 #include <erl_nif.h>
 
-#include <chrono>
+#include <ctime>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -42,8 +42,14 @@ struct Pending {
     ErlNifPid pid;
     ErlNifEnv *env;  // holds the copy of the caller's ref
     ERL_NIF_TERM ref;
-    std::chrono::steady_clock::time_point deadline;
+    uint64_t deadline_ns;  // CLOCK_MONOTONIC, the clock of nxs_request_done_ns
 };
+
+uint64_t monotonic_ns() {
+    timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return (uint64_t)t.tv_sec * 1000000000ull + (uint64_t)t.tv_nsec;
+}
 
 struct Context {
     nxs_context *context = nullptr;
@@ -102,7 +108,11 @@ ERL_NIF_TERM error_term(ErlNifEnv *env, void *arg) {
     return error(env, *reason == ":timeout" ? atom(env, "timeout") : text(env, *reason));
 }
 
-// The context's waiter: the head run, until done or past its deadline.
+// The context's waiter: the head run, until done or past its deadline. A run
+// is late when the device finished it (its outputs on the host) after its
+// deadline, or has not finished it by then, however soon the waiter looks:
+// the reply's arrival against the deadline, as the Matcher's mailbox orders
+// a Port reply and its deadline message.
 void wait_for_runs(Context *c) {
     std::unique_lock<std::mutex> l(c->lock);
     for (;;) {
@@ -110,11 +120,12 @@ void wait_for_runs(Context *c) {
         if (c->pending.empty()) return;  // stopping with nothing left
         Pending head = c->pending.front();
         l.unlock();
-        const auto now = std::chrono::steady_clock::now();
+        const uint64_t now = monotonic_ns();
         const long long left =
-            std::chrono::duration_cast<std::chrono::milliseconds>(head.deadline - now).count();
+            head.deadline_ns > now ? (long long)((head.deadline_ns - now + 999999) / 1000000) : 0;
         char why[512] = "";
-        const nxs_status s = nxs_request_wait(head.request, left > 0 ? left : 0, why, sizeof why);
+        nxs_status s = nxs_request_wait(head.request, left, why, sizeof why);
+        if (s == NXS_OK && nxs_request_done_ns(head.request) > head.deadline_ns) s = NXS_TIMEOUT;
         l.lock();
         if (s == NXS_TIMEOUT) {
             // Late: fail it and every run behind it, then let the device finish them.
@@ -255,7 +266,7 @@ ERL_NIF_TERM run_nif(ErlNifEnv *env, int, const ERL_NIF_TERM argv[]) {
         return error(env, text(env, "segment " + std::to_string(q.segment) + " is not configured"));
     if (s != NXS_OK) return error(env, text(env, buf));
     Pending p{request, pid, enif_alloc_env(), 0,
-              std::chrono::steady_clock::now() + std::chrono::milliseconds(timeout_ms)};
+              monotonic_ns() + (uint64_t)timeout_ms * 1000000ull};
     p.ref = enif_make_copy(p.env, argv[3]);
     {
         std::lock_guard<std::mutex> l(c->lock);

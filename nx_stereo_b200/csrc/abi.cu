@@ -447,6 +447,16 @@ extern "C" uint32_t nxs_path_words(uint32_t disparities) {
     return (uint32_t)path_words((int)disparities);
 }
 
+extern "C" nxs_status nxs_set_path_sums(uint32_t mode) {
+    if (mode > 1) return NXS_BAD_ARGUMENT;
+    set_path_sums((int)mode);
+    return NXS_OK;
+}
+
+extern "C" uint32_t nxs_path_sums(uint32_t width, uint32_t height, uint32_t disparities) {
+    return path_sums_wanted((int)width, (int)height, (int)disparities) ? 1u : 0u;
+}
+
 extern "C" uint64_t nxs_sgm_scratch_bytes(uint32_t width, uint32_t height, uint32_t disparities) {
     return matcher_scratch_bytes((int)width, (int)height, (int)disparities);
 }
@@ -786,6 +796,31 @@ extern "C" nxs_status nxs_select_paths_device_ordered(const uint8_t *d_paths, ui
                (paths == 3 || paths == 8) && (span == 0 || span == 8 || span == 16));
     return launch_select_paths(d_paths, width, height, disparities, paths, uniqueness,
                                d_disparity, d_keys, static_cast<cudaStream_t>(stream), (int)span)
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_path_sums_device(const uint8_t *d_costs, uint32_t width,
+                                           uint32_t height, uint32_t disparities, uint32_t paths,
+                                           uint32_t p1, uint32_t p2, uint16_t *d_sums,
+                                           void *stream) {
+    CHECK_SIZE(d_costs && d_sums && width > 0 && height > 0 && disparities % 16 == 0 &&
+               disparities >= 64 && disparities <= 256 && (paths == 3 || paths == 8) &&
+               p1 < p2 && p2 + 48 <= 127);
+    return launch_paths_sums(d_costs, width, height, disparities, paths, p1, p2, d_sums,
+                             static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_select_path_sums_device(const uint16_t *d_sums, uint32_t width,
+                                                  uint32_t height, uint32_t disparities,
+                                                  float uniqueness, float *d_disparity,
+                                                  uint32_t *d_keys, void *stream) {
+    CHECK_SIZE(d_sums && d_disparity && d_keys && width > 0 && height > 0 &&
+               disparities % 16 == 0 && disparities >= 64 && disparities <= 256);
+    return launch_select_path_sums(d_sums, width, height, disparities, uniqueness, d_disparity,
+                                   d_keys, static_cast<cudaStream_t>(stream))
                ? NXS_CUDA_ERROR
                : NXS_OK;
 }

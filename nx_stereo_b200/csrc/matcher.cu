@@ -103,7 +103,8 @@ cudaError_t launch_census_costs(const uint8_t *left, const uint8_t *right, int w
 
 // ---------------------------------------------------------------- paths
 // One warp per block, so blocks go to SMs as they free up, longest lines first.
-template <int G, int WORDS, bool FULL, int SPAN>
+// SUMS: every direction adds into one u16 aggregate volume (follow_lines).
+template <int G, int WORDS, bool FULL, int SPAN, bool SUMS = false>
 __global__ void __launch_bounds__(32)
     paths_kernel(const uint8_t *__restrict__ costs, uint8_t *__restrict__ paths_out,
                  const PathSetup s) {
@@ -111,8 +112,16 @@ __global__ void __launch_bounds__(32)
     using Piece = typename std::conditional<WORDS == 4, uint2, uint4>::type;
     constexpr int PIECES = WORDS == 16 ? 2 : 1;
     __shared__ Piece ring[kPrefetch * PIECES][32];
-    path_warp<G, WORDS, FULL, SPAN>(costs, paths_out, s, blockIdx.x, threadIdx.x,
-                                    &ring[0][threadIdx.x]);
+    path_warp<G, WORDS, FULL, SPAN, SUMS>(costs, paths_out, s, blockIdx.x, threadIdx.x,
+                                          &ring[0][threadIdx.x]);
+}
+
+// Zeroes `chunks` 16-byte chunks (the aggregate volume before the summing scan).
+__global__ void __launch_bounds__(256) clear_kernel(uint4 *__restrict__ to, size_t chunks) {
+    follow_previous_grid();
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < chunks; i += stride)
+        to[i] = make_uint4(0, 0, 0, 0);
 }
 
 // Words a path lane holds at each disparity count (4, 8 or 16), the tunable
@@ -228,6 +237,43 @@ cudaError_t launch_paths(const uint8_t *costs, int width, int height, int dispar
     return cudaGetLastError();
 }
 
+// How the matcher aggregates: 0 (the default) the path volumes, then
+// selection over all of them; 1 the summing scan into one aggregate volume,
+// then selection over it. The reductions run at a few TB/s in L2, below what
+// the path volumes' plain stores reach, so 1 measured slower at every size
+// from 364x272x64 to 1920x1080x256 and is kept as a knob, not a default.
+static int g_path_sums = 0;
+void set_path_sums(int mode) { g_path_sums = mode == 1 ? 1 : 0; }
+int path_sums_mode() { return g_path_sums; }
+
+bool path_sums_wanted(int width, int height, int disparities) {
+    (void)width;
+    (void)height;
+    return g_path_sums == 1 && disparities % 16 == 0 && path_words(disparities) == 8;
+}
+
+cudaError_t launch_paths_sums(const uint8_t *costs, int width, int height, int disparities,
+                              int paths, int p1, int p2, uint16_t *sums, cudaStream_t stream) {
+    if (disparities % 16 != 0) return cudaErrorInvalidValue;
+    const int g = path_lanes(disparities, 8);
+    if (g < 4 || g > 16) return cudaErrorInvalidValue;
+    const size_t chunks = (size_t)width * height * disparities * 2 / 16;
+    cudaError_t e = launch_after(clear_kernel, dim3(4 * 148), dim3(256), 0, stream,
+                                 reinterpret_cast<uint4 *>(sums), chunks);
+    if (e != cudaSuccess) return e;
+    PathSetup s;
+    const int total = path_setup(width, height, disparities, paths, p1, p2, g, &s);
+    const bool full = g * 16 == disparities;
+    uint8_t *out = reinterpret_cast<uint8_t *>(sums);
+#define NXS_SUMS(G, F)                                                                         \
+    launch_after(paths_kernel<G, 8, F, 16, true>, dim3(total), dim3(32), 0, stream, costs, out, s)
+    if (g == 4) full ? NXS_SUMS(4, true) : NXS_SUMS(4, false);
+    else if (g == 8) full ? NXS_SUMS(8, true) : NXS_SUMS(8, false);
+    else full ? NXS_SUMS(16, true) : NXS_SUMS(16, false);
+#undef NXS_SUMS
+    return cudaGetLastError();
+}
+
 // sums[y][x][d] = sum of the P path volumes, u16 (at most 8 x 127 = 1016).
 __global__ void sum_paths_kernel(const uint8_t *__restrict__ paths_in, size_t volume, int paths,
                                  uint16_t *__restrict__ sums) {
@@ -305,6 +351,13 @@ cudaError_t launch_select_sums(const uint16_t *sums, int width, int height, int 
                                cudaStream_t stream) {
     return launch_select<0>(sums, width, height, disparities, uniqueness, disparity, keys,
                             stream);
+}
+
+cudaError_t launch_select_path_sums(const uint16_t *sums, int width, int height,
+                                    int disparities, float uniqueness, float *disparity,
+                                    uint32_t *keys, cudaStream_t stream) {
+    return launch_select<-1, 16>(sums, width, height, disparities, uniqueness, disparity, keys,
+                                 stream);
 }
 
 // ---------------------------------------------------------------- check
@@ -484,6 +537,17 @@ cudaError_t run_matcher(const uint8_t *left, const uint8_t *right, int width, in
     const int span = matcher_span(disparities);
     if ((e = launch_census_costs(left, right, width, height, disparities, s.costs, stream, span)))
         return e;
+    if (path_sums_wanted(width, height, disparities)) {  // the aggregate in the path volumes' room
+        uint16_t *sums = reinterpret_cast<uint16_t *>(s.paths);
+        if ((e = launch_paths_sums(s.costs, width, height, disparities, paths, p1, p2, sums,
+                                   stream)))
+            return e;
+        if ((e = launch_select_path_sums(sums, width, height, disparities, uniqueness,
+                                         s.selected, s.keys, stream)))
+            return e;
+        return launch_check_median(s.selected, s.keys, width, height, stage_mask, disparity,
+                                   stream);
+    }
     if ((e = launch_paths(s.costs, width, height, disparities, paths, p1, p2, s.paths, stream,
                           span)))
         return e;

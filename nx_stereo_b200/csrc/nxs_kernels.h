@@ -43,6 +43,20 @@ cudaError_t launch_paths(const uint8_t *costs, int width, int height, int dispar
 // The order the matcher keeps its costs and path volumes in at this many
 // disparities: 8 with 4 words a path lane, 16 otherwise.
 int matcher_span(int disparities);
+// The summing path scan: the aggregate volume (u16, the lane-split layout of
+// sum_position in span-16 order, D a multiple of 16) zeroed, then every
+// direction's path costs added into it; selection over it with
+// launch_select_path_sums.
+cudaError_t launch_paths_sums(const uint8_t *costs, int width, int height, int disparities,
+                              int paths, int p1, int p2, uint16_t *sums, cudaStream_t stream);
+cudaError_t launch_select_path_sums(const uint16_t *sums, int width, int height,
+                                    int disparities, float uniqueness, float *disparity,
+                                    uint32_t *keys, cudaStream_t stream);
+// Whether the matcher aggregates with the summing scan at this size, by the
+// mode of set_path_sums (0 never, the default; 1 where the layout allows).
+bool path_sums_wanted(int width, int height, int disparities);
+void set_path_sums(int mode);
+int path_sums_mode();
 // sums[y][x][d] = sum over paths of paths_in (u16).
 cudaError_t launch_sum_paths(const uint8_t *paths_in, int width, int height, int disparities,
                              int paths, uint16_t *sums, cudaStream_t stream);

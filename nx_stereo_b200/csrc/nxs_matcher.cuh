@@ -467,6 +467,25 @@ __device__ __forceinline__ void copy_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// Adds four u16x2 words (eight u16 values below 1024) into 16 bytes of an
+// aggregate volume in L2: a vector f16x2 reduction on their bit patterns,
+// which for subnormals kept as such (.noftz) is the integer add.
+__device__ __forceinline__ void add_sums16(void *global, uint32_t a, uint32_t b, uint32_t c,
+                                           uint32_t d) {
+    asm volatile("red.relaxed.gpu.global.add.noftz.v4.f16x2 [%0], {%1, %2, %3, %4};\n" ::"l"(global),
+                 "r"(a), "r"(b), "r"(c), "r"(d)
+                 : "memory");
+}
+
+// Where the aggregate volume of the summing path scan keeps disparity
+// position j of a pixel (j in the span-16 permuted order of span_disparity,
+// lane j / 16 holding positions 16 * lane ..): the lane's words 0-3 (positions
+// 0-7 of its run) at u16 8 * lane + (j % 8), its words 4-7 at D / 2 + 8 * lane
+// + (j % 8).
+__host__ __device__ constexpr int sum_position(int disparities, int j) {
+    return (j % 16 < 8 ? 0 : disparities / 2) + 8 * (j / 16) + j % 8;
+}
+
 // The lines of one warp: G lanes per line, WORDS (4, 8 or 16) u16x2 words,
 // so 2 x WORDS disparities, per lane. `ring` is this thread's first slot of
 // the warp's kPrefetch x THREADS slots of 2 x WORDS bytes. SPAN (8 or 16, at
@@ -476,13 +495,23 @@ __device__ __forceinline__ void copy_wait() {
 // words k - 1 and k + 1, but for the first and last word of a run, whose
 // outer neighbour lies in the next run (one byte permute each); SPAN 0:
 // word k holds (2k, 2k + 1) and every neighbour is made by a byte permute.
-template <int G, int WORDS, bool FULL, int THREADS, int SPAN = 0>
+//
+// SUMS: instead of its own u8 volume, each direction adds its path costs into
+// one u16 aggregate volume (zeroed before the launch) in the lane-split
+// layout of sum_position, with 16-byte reductions: every direction's lane
+// sends its words 0-3 and 4-7 as two reductions, so G lanes cover two runs of
+// 16 * G contiguous bytes. The reductions are f16x2 adds on the u16 bit
+// patterns: an integer n < 1024 is the f16 subnormal n * 2^-24, and the sum
+// of subnormals below 2^-14 is exact with subnormals kept (.noftz), so the
+// adds are the integer adds (8 directions x at most 127 = 1016).
+template <int G, int WORDS, bool FULL, int THREADS, int SPAN = 0, bool SUMS = false>
 __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
                                              uint8_t *__restrict__ out, const PathSetup &s,
                                              int p, int line, int member, void *ring_base) {
     static_assert(WORDS == 4 || WORDS == 8 || WORDS == 16, "4, 8 or 16 words a lane");
     static_assert(SPAN == 0 || (SPAN >= 8 && SPAN <= 2 * WORDS && (2 * WORDS) % SPAN == 0),
                   "a lane holds whole permuted runs");
+    static_assert(!SUMS || WORDS == 8, "the aggregate layout has 16 disparities a lane");
     constexpr int BYTES = 2 * WORDS;             // a lane's disparities, one byte each
     constexpr int PIECE = BYTES < 16 ? BYTES : 16;  // bytes of one async copy
     constexpr int PIECES = BYTES / PIECE;
@@ -498,7 +527,9 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
     const int stride32 = (int)stride;
     const size_t at = ((size_t)y0 * W + x0) * D + member * BYTES;
     const uint8_t *ahead = costs + at;
-    uint8_t *dst = out + (size_t)p * s.volume + at;
+    // SUMS: lane `member`'s words 0-3 at u16 (pixel * D + 8 * member), 4-7 D bytes on.
+    uint8_t *dst = SUMS ? out + 2 * (((size_t)y0 * W + x0) * D + 8 * member)
+                        : out + (size_t)p * s.volume + at;
     const int steps = (int)__reduce_max_sync(kFullMask, (unsigned)length);
 
     uint32_t r[WORDS];
@@ -543,6 +574,9 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
             uint32_t from_right = __shfl_down_sync(kFullMask, r[0], 1);
             if (member == 0) from_left = kInf2;
             if (member == G - 1) from_right = kInf2;
+#ifdef NXS_PATH_IADD3
+            const uint32_t negm2 = 0u - m2;
+#endif
             uint32_t below[WORDS], above[WORDS];  // word k's values at d - 1 and at d + 1
             if constexpr (SPAN != 0) {
 #pragma unroll
@@ -580,19 +614,28 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
                 const uint32_t neighbour = vmin2(below[k], above[k]);
                 const uint32_t raised = mad_lo(neighbour, s.one, p1x2);
                 const uint32_t t = __vimin3_u16x2(r[k], j2, raised);
+#ifdef NXS_PATH_IADD3
+                const uint32_t value = t + cost[k] + negm2;
+#else
                 const uint32_t value = mad_lo(t, s.one, mad_lo(m2, s.minus_one, cost[k]));
+#endif
                 r[k] = (FULL || active) ? value : kInf2;
             }
             if (!CHECKED || (active && step < length)) {
+                if constexpr (SUMS) {
+                    add_sums16(dst, r[0], r[1], r[2], r[3]);
+                    add_sums16(dst + D, r[4], r[5], r[6], r[7]);
+                } else {
 #pragma unroll
-                for (int c = 0; c < PIECES; ++c) {
-                    if constexpr (PIECE == 16)
-                        __stcs(reinterpret_cast<uint4 *>(dst + 16 * c), pack16(r + 8 * c));
-                    else
-                        __stcs(reinterpret_cast<uint2 *>(dst + 8 * c), pack8(r + 4 * c));
+                    for (int c = 0; c < PIECES; ++c) {
+                        if constexpr (PIECE == 16)
+                            __stcs(reinterpret_cast<uint4 *>(dst + 16 * c), pack16(r + 8 * c));
+                        else
+                            __stcs(reinterpret_cast<uint2 *>(dst + 8 * c), pack8(r + 4 * c));
+                    }
                 }
             }
-            dst = advance(dst, stride32, s.one);
+            dst = advance(dst, SUMS ? 2 * stride32 : stride32, s.one);
             // The lowest path cost over the line's disparities: a shallow tree
             // over the lane's words, both halves folded into each half, then
             // over the line's G lanes a shuffle tree (one warp-wide reduction
@@ -661,7 +704,7 @@ __host__ __device__ __forceinline__ int ranked_line(int rank, int dy, int dx, in
 // Rows, then columns, then the diagonals of all four directions by rank.
 // `ring`: this lane's first slot of the warp's kPrefetch x 32 slots of
 // 2 x WORDS bytes (in pieces of at most 16 bytes, strided by 32 lanes).
-template <int G, int WORDS, bool FULL, int SPAN = 0>
+template <int G, int WORDS, bool FULL, int SPAN = 0, bool SUMS = false>
 __device__ __forceinline__ void path_warp(const uint8_t *__restrict__ costs,
                                           uint8_t *__restrict__ paths_out, const PathSetup &s,
                                           int warp, int lane, void *ring) {
@@ -680,7 +723,7 @@ __device__ __forceinline__ void path_warp(const uint8_t *__restrict__ costs,
     const int rank = group * (32 / G) + lane / G;
     const int line =
         rank < s.lines[p] ? ranked_line(rank, s.dy[p], s.dx[p], s.width, s.height) : rank;
-    follow_lines<G, WORDS, FULL, 32, SPAN>(costs, paths_out, s, p, line, lane % G, ring);
+    follow_lines<G, WORDS, FULL, 32, SPAN, SUMS>(costs, paths_out, s, p, line, lane % G, ring);
 }
 
 // Lanes per pixel (selection) or per line (paths with 16 disparities a lane),
@@ -712,7 +755,9 @@ __host__ __device__ inline int path_lanes(int disparities, int words) {
 // (65535 - d) (lib/nx_stereo.ex:646-664). `values_of` is 128 / G rows of 256
 // values in shared memory.
 // SPAN: the path volumes' disparity order (span_disparity).
-template <int G, int PATHS, int SPAN = 0>  // PATHS 0: u16 sums, not path volumes
+// PATHS 0: u16 sums in the volumes' order, not path volumes; -1: u16 sums in
+// the lane-split layout of sum_position (the summing path scan's output).
+template <int G, int PATHS, int SPAN = 0>
 __device__ __forceinline__ void select_pixels(const void *__restrict__ source, int width,
                                               int height, int disparities, size_t volume,
                                               float uniqueness, float *__restrict__ disparity,
@@ -734,9 +779,12 @@ __device__ __forceinline__ void select_pixels(const void *__restrict__ source, i
     for (int k = 0; k < 8; ++k) v[k] = 0;
     if (active) {
         const size_t at = pixel * D + d0;
-        if (PATHS == 0) {
-            const uint4 *sums = reinterpret_cast<const uint4 *>(static_cast<const uint16_t *>(source) + at);
-            const uint4 a = __ldcg(sums), b = __ldcg(sums + 1);
+        if (PATHS <= 0) {
+            const uint16_t *base = static_cast<const uint16_t *>(source);
+            const uint4 *sums = reinterpret_cast<const uint4 *>(
+                PATHS == 0 ? base + at : base + pixel * D + 8 * member);
+            const uint4 a = __ldcg(sums);
+            const uint4 b = __ldcg(PATHS == 0 ? sums + 1 : sums + D / 16);
             v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
             v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
         } else {

@@ -127,6 +127,8 @@ SIGNATURES = {
     "nxs_sgm_scratch_bytes": (_u64, [_u32, _u32, _u32]),
     "nxs_set_path_words": (_i, [_u32, _u32]),
     "nxs_path_words": (_u32, [_u32]),
+    "nxs_set_path_sums": (_i, [_u32]),
+    "nxs_path_sums": (_u32, [_u32, _u32, _u32]),
     "nxs_band_check": (_i, [ctypes.POINTER(BandParams), _u32, _u32, ctypes.c_int32] + _err),
     "nxs_band_scratch_bytes": (_u64, [_u32, _u32, _u32, ctypes.c_int32]),
     "nxs_sgm_band_device": (_i, [_P, _P, _P, _P, _u32, _u32, ctypes.POINTER(BandParams), _P, _P]
@@ -148,6 +150,8 @@ SIGNATURES = {
     "nxs_census_costs_device_ordered": (_i, [_P, _P, _u32, _u32, _u32, _u32, _P, _P]),
     "nxs_paths_device_ordered": (_i, [_P, _u32, _u32, _u32, _u32, _u32, _u32, _u32, _P, _P]),
     "nxs_select_paths_device_ordered": (_i, [_P, _u32, _u32, _u32, _u32, _f, _u32, _P, _P, _P]),
+    "nxs_path_sums_device": (_i, [_P, _u32, _u32, _u32, _u32, _u32, _u32, _P, _P]),
+    "nxs_select_path_sums_device": (_i, [_P, _u32, _u32, _u32, _f, _P, _P, _P]),
     "nxs_consistency_device": (_i, [_P, _P, _u32, _u32, _P, _P]),
     "nxs_median3_device": (_i, [_P, _u32, _u32, _u32, _P, _P]),
     "nxs_rectify_device": (_i, [_P, _u32, _u32, ctypes.POINTER(Camera), _u32, _u32, _P, _P]),

@@ -1,8 +1,8 @@
 """Builds the CPU oracle into oracle/_build/liboracle.so (test infrastructure).
 
-The reference itself (Elixir/Nx and a Rust crate) has no compiler in this
-image, so nothing under the reference is built; the oracle is this directory's
-C restatement. -ffp-contract=off keeps every f32 operation rounded on its own,
+The reference's Elixir/Nx and Rust code has no compiler in this image; the
+oracle is this directory's C restatement of it, and build_ref.py compiles
+the reference's compute shaders as C++ to pin that restatement. -ffp-contract=off keeps every f32 operation rounded on its own,
 in source order, as the reference evaluates it.
 """
 import os

@@ -46,14 +46,30 @@ def test_runs_reply_in_order_with_cuda_segments_outputs(nif):
                                         60000)
         for key in got:
             assert got[key].tobytes() == np.asarray(want[key]).astype(got[key].dtype).tobytes()
-    # a run past its timeout fails, and so does the one behind it
+    # A run past its timeout fails, and so does the one sent behind it. A
+    # large pair (ref 199, milliseconds of device work, a long timeout) holds
+    # the waiter while the late run (ref 200: as much work, a 1 ms timeout)
+    # and a small run behind it (ref 201) are sent: the device cannot finish
+    # ref 200 within 1 ms of its sending, so it is late however soon the
+    # waiter looks, and ref 201 is waiting behind it then.
+    big_geometry = segment.standard_geometry(4096, 2160)
+    status, big_members = segment.members([(stage.Disparity, {"num_disparities": 128})],
+                                          big_geometry)
+    status, big = segment.CudaSegment.build(big_members, big_geometry)
+    record = pc.configure_record(23, big_geometry, segment._configuration(big))
+    assert nif.text(nif.call("configure", ctx, nif.binary(record))) == ":ok"
+    big_left, big_right = scene.rectified_pair(4096, 2160, seed=7)
+    big_run = pc.run_record(23, big.inputs, [("left", big_left), ("right", big_right)])
     left, right = pairs[0]
     run = pc.run_record(21, seg.inputs, [("left", left), ("right", right)])
-    for k, timeout in enumerate((0, 30000)):
-        nif.call("run", ctx, nif.binary(run), nif.lib.fake_pid(9), nif.lib.fake_ref(200 + k),
-                 nif.lib.fake_int(timeout))
+    for ref, record, timeout in ((199, big_run, 30000), (200, big_run, 1), (201, run, 30000)):
+        assert nif.text(nif.call("run", ctx, nif.binary(record), nif.lib.fake_pid(9),
+                                 nif.lib.fake_ref(ref), nif.lib.fake_int(timeout))) == ":ok"
+    assert nif.message().startswith("#PID<9> {#Ref<199>, {:ok, ")
     assert nif.message() == "#PID<9> {#Ref<200>, {:error, :timeout}}"
     assert nif.message() == "#PID<9> {#Ref<201>, {:error, :timeout}}"
+    nif.call("release", ctx, nif.lib.fake_int(23))
+    big.release()
     # the owner's exit releases the segment
     assert nif.text(nif.call("watch", ctx, nif.lib.fake_pid(9), nif.lib.fake_int(21))) == ":ok"
     nif.lib.fake_process_down(9)
