@@ -16,7 +16,8 @@ rectified pairs of mixed sizes and disparity ranges in one persistent,
 graph-captured launch, against the single-pair matcher on the same pairs),
 `large_range` (8 pairs of 1920x1080 at 256 disparities), `coarse_to_fine`
 (Stage.Disparity's coarse-to-fine search at 728x544, band 16, beside the full
-search) and `serving` (32 camera streams with Poisson arrivals at 30 pairs/s
+search), `config0` (the 364x272, 64-disparity matcher, beside the CPU port)
+and `serving` (32 camera streams with Poisson arrivals at 30 pairs/s
 each: p50/p99 latency).
 
 `--impl reference` times the reference's CPU formulation of the same pipeline
@@ -71,6 +72,12 @@ def parse():
     p.add_argument("--no-batch", action="store_true", help="skip the batched workload")
     p.add_argument("--no-serving", action="store_true", help="skip the serving workload")
     p.add_argument("--no-large", action="store_true", help="skip the large-range workload")
+    p.add_argument("--aggregate", default="volumes", choices=["volumes", "sums"],
+                   help="the device pipeline's aggregation: 8 path volumes summed by selection "
+                        "(the default), or every direction adding into one u16 volume")
+    p.add_argument("--path-tiles", type=int, default=1, choices=[0, 1, 2],
+                   help="path scans take their costs by bulk tensor copies: 0 never, 2 always, "
+                        "1 for large pairs (the library's default)")
     p.add_argument("--no-coarse-to-fine", action="store_true",
                    help="skip the coarse-to-fine workload")
     return p.parse_args()
@@ -160,10 +167,11 @@ class DevicePipeline:
     """The pipeline's kernels on device buffers, one C-ABI call per stage; CUDA
     events bracket the path-aggregation kernel (the dominant one)."""
 
-    def __init__(self, native, torch, ctx, rig, stream):
+    def __init__(self, native, torch, ctx, rig, stream, aggregate="volumes"):
         from nx_stereo_b200 import scene
 
         self.native, self.torch, self.ctx, self.stream = native, torch, ctx, stream
+        self.sums = aggregate == "sums"
         cams = scene.cameras(rig)
         self.cameras = [native.make_camera(cams[s]["k"], cams[s]["d"], cams[s]["inverse_pr"])
                         for s in ("left", "right")]
@@ -213,12 +221,20 @@ class DevicePipeline:
              self.images[1].data_ptr(), WIDTH, HEIGHT, DISPARITIES, self.span,
              self.costs.data_ptr(), s)
         mark(2)
-        call("nxs_paths_device_ordered", self.costs.data_ptr(), WIDTH, HEIGHT, DISPARITIES, PATHS,
-             8, 64, self.span, self.volumes.data_ptr(), s)
-        mark(3)
-        call("nxs_select_paths_device_ordered", self.volumes.data_ptr(), WIDTH, HEIGHT,
-             DISPARITIES, PATHS, 1.0526315789473684, self.span, self.selected.data_ptr(),
-             self.keys.data_ptr(), s)
+        if self.sums:  # every direction adds into one u16 volume (in the volumes' room)
+            call("nxs_path_sums_device", self.costs.data_ptr(), WIDTH, HEIGHT, DISPARITIES, PATHS,
+                 8, 64, self.volumes.data_ptr(), s)
+            mark(3)
+            call("nxs_select_path_sums_device", self.volumes.data_ptr(), WIDTH, HEIGHT,
+                 DISPARITIES, 1.0526315789473684, self.selected.data_ptr(), self.keys.data_ptr(),
+                 s)
+        else:
+            call("nxs_paths_device_ordered", self.costs.data_ptr(), WIDTH, HEIGHT, DISPARITIES,
+                 PATHS, 8, 64, self.span, self.volumes.data_ptr(), s)
+            mark(3)
+            call("nxs_select_paths_device_ordered", self.volumes.data_ptr(), WIDTH, HEIGHT,
+                 DISPARITIES, PATHS, 1.0526315789473684, self.span, self.selected.data_ptr(),
+                 self.keys.data_ptr(), s)
         mark(4)
         call("nxs_check_median_device", self.selected.data_ptr(), self.keys.data_ptr(), WIDTH,
              HEIGHT, 1, self.disparity.data_ptr(), s)
@@ -236,14 +252,14 @@ def run_ours(args, rank, world, local_rank):
     from nx_stereo_b200 import native, replicas, segment, stage
 
     torch.cuda.set_device(local_rank)
-    native.load()
+    native.load().nxs_set_path_tiles(args.path_tiles)
     ctx = native.Context(local_rank)
     rig, frames = make_inputs(args.inputs, seed=replicas.seed(rank, 0))
     stream_obj = torch.cuda.Stream()
 
     with torch.cuda.stream(stream_obj):
         s = stream_obj.cuda_stream
-        pipe = DevicePipeline(native, torch, ctx, rig, s)
+        pipe = DevicePipeline(native, torch, ctx, rig, s, args.aggregate)
         d_frames = [(torch.from_numpy(l).cuda(), torch.from_numpy(r).cuda()) for l, r in frames]
         flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
         for i in range(args.warmup):
@@ -326,6 +342,7 @@ def run_ours(args, rank, world, local_rank):
     gc.disable()
     try:
         e0 = time.perf_counter()
+        c0 = time.thread_time()  # the calling thread's CPU time: the API's host cost
         e2e_pairs = 0
         while True:
             e2e_loop(args.steps)
@@ -335,6 +352,7 @@ def run_ours(args, rank, world, local_rank):
             if not replicas.agree(more, device="cuda"):
                 break
         e_elapsed = time.perf_counter() - e0
+        host_cpu_s = time.thread_time() - c0
         e1 = time.monotonic()
     finally:
         if collecting:
@@ -380,9 +398,12 @@ def run_ours(args, rank, world, local_rank):
                 "unit": "pairs/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "pairs": e2e_pairs, "seconds": round(e_s, 3),
+                "host_cpu_us_per_pair": round(1e6 * host_cpu_s / e2e_pairs, 1),
                 "api": "CudaSegment.send_request/await_ (C ABI nxs_run_async), depth "
                        f"{mod.depth()}, cyclic garbage collector paused while timed"},
         "clocks": clocks,
+        "aggregate": args.aggregate,
+        "path_tiles": args.path_tiles,
     }
     return line
 
@@ -678,6 +699,53 @@ def bench_coarse_to_fine(torch, ctx, pairs=64):
                       "pairs outside the events"}
 
 
+def bench_config0(torch, ctx, pairs=200):
+    """The plain single-pair matcher on the 364x272, 64-disparity, 8-path pair
+    (NxStereo.sgm/3: census, costs, paths, selection, check, median), device
+    buffers, CUDA events around each pair with L2 flushed between pairs; beside
+    it the C port of the reference's Rust matcher on every host thread."""
+    from nx_stereo_b200 import scene
+    from oracle import oracle
+
+    w, h, d = 364, 272, 64
+    inputs = [scene.rectified_pair(w, h, seed=400 + i, rectangles=6, max_disparity=56)
+              for i in range(8)]
+    devs = [(torch.from_numpy(l).cuda(), torch.from_numpy(r).cuda()) for l, r in inputs]
+    out = torch.empty((h, w), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    marks = []
+    with torch.cuda.stream(stream):
+        for i in range(pairs + 3):
+            dl, dr = devs[i % len(devs)]
+            flush.fill_(i & 0xFF)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ctx.sgm_device(dl.data_ptr(), dr.data_ptr(), w, h, out.data_ptr(),
+                           stream=stream.cuda_stream, disparities=d, paths=PATHS)
+            b.record(stream)
+            if i >= 3:
+                marks.append((a, b))
+    torch.cuda.synchronize()
+    ms = statistics.mean(a.elapsed_time(b) for a, b in marks)
+    exact = bool(np.array_equal(out.cpu().numpy().view(np.uint32),
+                                oracle.sgm(*inputs[(pairs + 2) % len(inputs)], d, PATHS)
+                                .view(np.uint32)))
+    threads = host_threads()
+    lefts = np.stack([inputs[i % len(inputs)][0] for i in range(threads)])
+    rights = np.stack([inputs[i % len(inputs)][1] for i in range(threads)])
+    t = time.perf_counter()
+    oracle.fast_sgm_batch(lefts, rights, d, PATHS, threads=threads)
+    cpu = threads / (time.perf_counter() - t)
+    return {"workload": "364x272 rectified pairs, D64, 8 paths, sgm/3 (check and median)",
+            "pairs": pairs, "ms_per_pair": round(ms, 4), "pairs_per_s": round(1000.0 / ms, 1),
+            "bit_exact_last_pair": exact,
+            "cpu_port_pairs_per_s": round(cpu, 2), "cpu_threads": threads,
+            "timing": "CUDA events around each pair on device buffers, L2 flushed between "
+                      "pairs outside the events"}
+
+
 def bench_serving(seconds=3.0, max_in_flight=SERVING_CAP):
     """32 camera streams (728x544 and 1280x720 alternating), Poisson arrivals
     at 30 pairs/s each, Rectification -> Disparity(128) -> SpeckleFilter ->
@@ -795,6 +863,8 @@ def main():
             line["large_range"] = bench_large(torch, ctx)
         if not args.no_coarse_to_fine:
             line["coarse_to_fine"] = bench_coarse_to_fine(torch, ctx)
+        if not args.no_cpu_baseline:
+            line["config0"] = bench_config0(torch, ctx)
         ctx.close()
         if not args.no_serving:
             line["serving"] = bench_serving()

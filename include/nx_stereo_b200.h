@@ -210,6 +210,19 @@ uint32_t nxs_path_words(uint32_t disparities);
 nxs_status nxs_set_path_sums(uint32_t mode);
 uint32_t nxs_path_sums(uint32_t width, uint32_t height, uint32_t disparities);
 
+/* How the path scans stream the cost volume: with tiles, the blocks of 8
+ * steps that every line of a warp covers come as bulk tensor copies, one
+ * [8][D] tile a line, into shared memory; without, every lane copies its own
+ * 16 bytes a step. Mode 0 never tiles, 2 always, 1 (the default) from 96 Mi
+ * pixel-disparities a pair on (1280x720 at 128 and up), where tiles measured
+ * faster. A tuning knob for the whole library; results do not depend on it.
+ * nxs_path_wait_failures: the path scans' waits on those copies that gave up
+ * on the current device (each wait is bounded, about 1 s; 0 unless a copy
+ * never landed, after which that launch's path volumes are incomplete). */
+nxs_status nxs_set_path_tiles(uint32_t mode);
+uint32_t nxs_path_tiles(void);
+uint32_t nxs_path_wait_failures(void);
+
 /* The disparity of each left pixel, -1.0 where unmatched: NxStereo.sgm/3 on a
  * rectified u8 pair in host memory (lib/nx_stereo.ex:64-74; natively
  * Matcher::disparity, native/stereo_match/src/lib.rs:105-124). Synchronous. */

@@ -457,6 +457,16 @@ extern "C" uint32_t nxs_path_sums(uint32_t width, uint32_t height, uint32_t disp
     return path_sums_wanted((int)width, (int)height, (int)disparities) ? 1u : 0u;
 }
 
+extern "C" nxs_status nxs_set_path_tiles(uint32_t mode) {
+    if (mode > 2) return NXS_BAD_ARGUMENT;
+    set_path_tiles((int)mode);
+    return NXS_OK;
+}
+
+extern "C" uint32_t nxs_path_tiles(void) { return (uint32_t)path_tiles(); }
+
+extern "C" uint32_t nxs_path_wait_failures(void) { return path_wait_failures(); }
+
 extern "C" uint64_t nxs_sgm_scratch_bytes(uint32_t width, uint32_t height, uint32_t disparities) {
     return matcher_scratch_bytes((int)width, (int)height, (int)disparities);
 }

@@ -13,8 +13,9 @@
 // D = 128.
 #include <algorithm>
 #include <mutex>
-
 #include <type_traits>
+
+#include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
 
 #include "nxs_kernels.h"
 #include "nxs_matcher.cuh"
@@ -104,16 +105,89 @@ cudaError_t launch_census_costs(const uint8_t *left, const uint8_t *right, int w
 // ---------------------------------------------------------------- paths
 // One warp per block, so blocks go to SMs as they free up, longest lines first.
 // SUMS: every direction adds into one u16 aggregate volume (follow_lines).
-template <int G, int WORDS, bool FULL, int SPAN, bool SUMS = false>
+// TILES: the blocks of steps every line of a warp covers take their costs by
+// bulk tensor copies of `maps` into kTileStages stages of 8 steps x 32 lanes
+// x 16 bytes; the per-lane ring of the other steps shares the first stage.
+template <int G, int WORDS, bool FULL, int SPAN, bool SUMS = false, bool TILES = false>
 __global__ void __launch_bounds__(32)
     paths_kernel(const uint8_t *__restrict__ costs, uint8_t *__restrict__ paths_out,
-                 const PathSetup s) {
-    follow_previous_grid();
+                 const PathSetup s, const __grid_constant__ CostMaps maps) {
     using Piece = typename std::conditional<WORDS == 4, uint2, uint4>::type;
     constexpr int PIECES = WORDS == 16 ? 2 : 1;
-    __shared__ Piece ring[kPrefetch * PIECES][32];
-    path_warp<G, WORDS, FULL, SPAN, SUMS>(costs, paths_out, s, blockIdx.x, threadIdx.x,
-                                          &ring[0][threadIdx.x]);
+    constexpr int RING_BYTES = kPrefetch * PIECES * 32 * (int)sizeof(Piece);
+    constexpr int TILE_BYTES = kTileStages * kPrefetch * 32 * 16;
+    static_assert(!TILES || RING_BYTES <= TILE_BYTES / kTileStages, "the ring fits one stage");
+    __shared__ __align__(128) uint8_t room[TILES ? TILE_BYTES : RING_BYTES];
+    __shared__ __align__(8) uint64_t bars[TILES ? kTileStages : 1];
+    if constexpr (TILES) {
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < kTileStages; ++k) barrier_init(&bars[k], 32 / G);
+            barrier_init_fence();
+        }
+        __syncwarp();
+    }
+    follow_previous_grid();
+    path_warp<G, WORDS, FULL, SPAN, SUMS, TILES>(costs, paths_out, s, blockIdx.x, threadIdx.x,
+                                                 reinterpret_cast<Piece *>(room) + threadIdx.x,
+                                                 &maps, room, bars);
+}
+
+// ---- the cost volume's tensor maps (cuTensorMapEncodeTiled, from the driver) ----
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult found;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &found) ==
+                cudaSuccess &&
+            found == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    });
+    return encode;
+}
+
+// The four views of a [H][W][D] u8 cost volume that CostMaps describes; false
+// where the driver refuses one (then the scan takes the per-lane copies).
+static bool encode_cost_maps(const uint8_t *costs, int width, int height, int disparities,
+                             CostMaps *maps) {
+    const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (!encode || width < 2 || height < 2) return false;
+    const cuuint64_t D = (cuuint64_t)disparities;
+    const cuuint64_t pixels = (cuuint64_t)width * (cuuint64_t)height;
+    auto view = [&](CUtensorMap *map, cuuint64_t step_pixels) {
+        const cuuint64_t dims[3] = {D, (cuuint64_t)kPrefetch, pixels};
+        const cuuint64_t strides[2] = {step_pixels * D, D};  // bytes, of dimensions 1 and 2
+        const cuuint32_t box[3] = {(cuuint32_t)D, (cuuint32_t)kPrefetch, 1};
+        const cuuint32_t element_strides[3] = {1, 1, 1};
+        return encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t *>(costs), dims,
+                      strides, box, element_strides, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    };
+    const cuuint64_t W = (cuuint64_t)width;
+    return view(&maps->row, 1) && view(&maps->column, W) && view(&maps->diagonal, W + 1) &&
+           view(&maps->anti, W - 1);
+}
+
+// Whether the path scans take their full blocks' costs by tensor copies: 0
+// never, 2 always, 1 (the default) from kTilesFrom pixel-disparities on,
+// where they measured faster (1280x720x128: 295 against 300 us, 1920x1080x256:
+// 1329 against 1360 us); below it the per-lane copies were (728x544x128: 121
+// against 129 us, 364x272x64: 40 against 53 us). Results do not depend on it.
+static int g_path_tiles = 1;
+constexpr size_t kTilesFrom = (size_t)96 << 20;
+void set_path_tiles(int mode) { g_path_tiles = mode < 0 || mode > 2 ? 1 : mode; }
+int path_tiles() { return g_path_tiles; }
+static bool tiles_wanted(int width, int height, int disparities) {
+    return g_path_tiles == 2 ||
+           (g_path_tiles == 1 && (size_t)width * height * disparities >= kTilesFrom);
+}
+
+unsigned path_wait_failures() {
+    unsigned n = 0;
+    if (cudaMemcpyFromSymbol(&n, g_path_wait_failures, sizeof n) != cudaSuccess) return ~0u;
+    return n;
 }
 
 // Zeroes `chunks` 16-byte chunks (the aggregate volume before the summing scan).
@@ -148,7 +222,6 @@ int path_setup(int width, int height, int disparities, int paths, int p1, int p2
     s.paths = paths;
     s.volume = (size_t)width * height * disparities;
     s.one = 1u;
-    s.minus_one = 0xFFFFFFFFu;
     const int lines_per_warp = 32 / lanes;
     // Rows, then columns, then diagonals.
     int n = 0;
@@ -189,9 +262,23 @@ static void launch_paths_in(const uint8_t *costs, uint8_t *paths_out, const Path
                             int total, int g, cudaStream_t stream) {
     constexpr int SPAN = PERMUTED ? (WORDS == 4 ? 8 : 16) : 0;
     const bool full = g * 2 * WORDS == s.disparities;
+    CostMaps maps{};
+    if constexpr (WORDS == 8 && PERMUTED) {
+        if (full && tiles_wanted(s.width, s.height, s.disparities) &&
+            encode_cost_maps(costs, s.width, s.height, s.disparities, &maps)) {
+#define NXS_TILED(G)                                                                           \
+    launch_after(paths_kernel<G, 8, true, 16, false, true>, dim3(total), dim3(32), 0, stream,  \
+                 costs, paths_out, s, maps)
+            if (g == 4) NXS_TILED(4);
+            else if (g == 8) NXS_TILED(8);
+            else NXS_TILED(16);
+#undef NXS_TILED
+            return;
+        }
+    }
 #define NXS_PATHS(G, F)                                                                        \
     launch_after(paths_kernel<G, WORDS, F, SPAN>, dim3(total), dim3(32), 0, stream, costs,    \
-                 paths_out, s)
+                 paths_out, s, maps)
     if constexpr (WORDS == 16) {
         if (g == 2) full ? NXS_PATHS(2, true) : NXS_PATHS(2, false);
         else if (g == 4) full ? NXS_PATHS(4, true) : NXS_PATHS(4, false);
@@ -265,8 +352,10 @@ cudaError_t launch_paths_sums(const uint8_t *costs, int width, int height, int d
     const int total = path_setup(width, height, disparities, paths, p1, p2, g, &s);
     const bool full = g * 16 == disparities;
     uint8_t *out = reinterpret_cast<uint8_t *>(sums);
+    const CostMaps maps{};
 #define NXS_SUMS(G, F)                                                                         \
-    launch_after(paths_kernel<G, 8, F, 16, true>, dim3(total), dim3(32), 0, stream, costs, out, s)
+    launch_after(paths_kernel<G, 8, F, 16, true>, dim3(total), dim3(32), 0, stream, costs, out, s, \
+                 maps)
     if (g == 4) full ? NXS_SUMS(4, true) : NXS_SUMS(4, false);
     else if (g == 8) full ? NXS_SUMS(8, true) : NXS_SUMS(8, false);
     else full ? NXS_SUMS(16, true) : NXS_SUMS(16, false);

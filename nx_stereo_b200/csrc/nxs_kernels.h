@@ -57,6 +57,14 @@ cudaError_t launch_select_path_sums(const uint16_t *sums, int width, int height,
 bool path_sums_wanted(int width, int height, int disparities);
 void set_path_sums(int mode);
 int path_sums_mode();
+// Whether the path scans take the costs of the blocks of steps every line of
+// a warp covers by bulk tensor copies: 0 never, 1 (the default) for large
+// pairs, 2 always.
+void set_path_tiles(int mode);
+int path_tiles();
+// The path scans' waits on their tensor copies that ran out of tries since
+// the library was loaded on this device (0 unless a copy never landed).
+unsigned path_wait_failures();
 // sums[y][x][d] = sum over paths of paths_in (u16).
 cudaError_t launch_sum_paths(const uint8_t *paths_in, int width, int height, int disparities,
                              int paths, uint16_t *sums, cudaStream_t stream);

@@ -7,6 +7,8 @@
 #include <cstdint>
 #include <type_traits>
 
+#include <cuda.h>  // CUtensorMap
+
 #include "nxs_device.cuh"
 
 namespace nxs {
@@ -167,17 +169,24 @@ __device__ __forceinline__ void census4_tile(const uint8_t *__restrict__ image, 
 // stores.
 constexpr int kCostPixels = 64;
 
-// The permuted disparity order: within each run of SPAN disparities, bytes 2k
-// and 2k + 1 hold disparities k and k + SPAN / 2, so the u16x2 word k of a
-// path lane holding SPAN disparities holds (k, k + SPAN / 2), and the
-// neighbours of both halves at d - 1 and at d + 1 are the whole words k - 1
-// and k + 1. SPAN 0 is the natural order. span_disparity: the disparity at
+// The permuted disparity order: a path lane holding a run of SPAN
+// disparities keeps them as u16x2 words, word k holding (k, k + SPAN / 2), so
+// the neighbours of both halves at d - 1 and at d + 1 are the whole words
+// k - 1 and k + 1. In memory each 4 bytes 4q .. 4q + 3 of a run hold words
+// 2q and 2q + 1 interleaved: disparities 2q, 2q + 1, 2q + SPAN / 2 and
+// 2q + 1 + SPAN / 2, so a lane packs two words into one u32 with one
+// multiply-add (w[2q] + 256 w[2q + 1]) and unpacks them with two byte
+// permutes. SPAN 0 is the natural order. span_disparity: the disparity at
 // byte j; span_position: the byte that holds disparity d.
 __host__ __device__ constexpr int span_disparity(int span, int j) {
-    return span == 0 ? j : (j / span) * span + (j % span) / 2 + (span / 2) * ((j % span) % 2);
+    return span == 0 ? j
+                     : (j / span) * span + 2 * ((j % span) / 4) + (j % 2) +
+                           (span / 2) * (((j % span) / 2) % 2);
 }
 __host__ __device__ constexpr int span_position(int span, int d) {
-    return span == 0 ? d : (d / span) * span + 2 * ((d % span) % (span / 2)) + (d % span) / (span / 2);
+    return span == 0 ? d
+                     : (d / span) * span + 4 * (((d % span) % (span / 2)) / 2) + (d % 2) +
+                           2 * ((d % span) / (span / 2));
 }
 
 // Where code j of a staged code array (lefts, rights below) lies: within each
@@ -371,9 +380,9 @@ struct PathSetup {
     int dy[8], dx[8];
     int order[8];       // direction of each slot: rows first, then columns, then diagonals
     int straight;       // slots of rows and columns
-    // 1 and 0xFFFFFFFF, given at run time so that the recurrence's adds are
-    // issued as multiply-adds on the FMA pipe (see follow_lines).
-    unsigned one, minus_one;
+    // 1, given at run time so that some of the recurrence's adds and the
+    // pointer steps are issued as multiply-adds on the FMA pipe (follow_lines).
+    unsigned one;
     size_t volume;      // bytes of one direction's volume
 };
 
@@ -390,6 +399,33 @@ __device__ __forceinline__ T *advance(T *p, int a, unsigned b) {
     uint64_t d;
     asm("mad.wide.s32 %0, %1, %2, %3;" : "=l"(d) : "r"(a), "r"((int)b), "l"((uint64_t)p));
     return reinterpret_cast<T *>(d);
+}
+
+// The words of a permuted run (span_disparity) from its bytes, and back.
+__device__ __forceinline__ void unpack_run16(const uint4 c, uint32_t *w) {
+    w[0] = __byte_perm(c.x, 0, 0x4240);
+    w[1] = __byte_perm(c.x, 0, 0x4341);
+    w[2] = __byte_perm(c.y, 0, 0x4240);
+    w[3] = __byte_perm(c.y, 0, 0x4341);
+    w[4] = __byte_perm(c.z, 0, 0x4240);
+    w[5] = __byte_perm(c.z, 0, 0x4341);
+    w[6] = __byte_perm(c.w, 0, 0x4240);
+    w[7] = __byte_perm(c.w, 0, 0x4341);
+}
+__device__ __forceinline__ void unpack_run8(const uint2 c, uint32_t *w) {
+    w[0] = __byte_perm(c.x, 0, 0x4240);
+    w[1] = __byte_perm(c.x, 0, 0x4341);
+    w[2] = __byte_perm(c.y, 0, 0x4240);
+    w[3] = __byte_perm(c.y, 0, 0x4341);
+}
+// Halves below 256: w[2q] + 256 w[2q + 1] interleaves their bytes (a
+// multiply-add by a run-time 256, on the FMA pipe).
+__device__ __forceinline__ uint4 pack_run16(const uint32_t *w, uint32_t byte) {
+    return make_uint4(mad_lo(w[1], byte, w[0]), mad_lo(w[3], byte, w[2]),
+                      mad_lo(w[5], byte, w[4]), mad_lo(w[7], byte, w[6]));
+}
+__device__ __forceinline__ uint2 pack_run8(const uint32_t *w, uint32_t byte) {
+    return make_uint2(mad_lo(w[1], byte, w[0]), mad_lo(w[3], byte, w[2]));
 }
 
 __device__ __forceinline__ void unpack16(const uint4 c, uint32_t *w) {
@@ -477,6 +513,83 @@ __device__ __forceinline__ void add_sums16(void *global, uint32_t a, uint32_t b,
                  : "memory");
 }
 
+// ---- bulk tensor copies of the cost stream ----
+// The cost volume [H][W][D] bytes seen four ways, one per kind of scan line:
+// a 3-D tensor map of (d, s, q) at byte q D + s S + d, S the line's step in
+// bytes (D for rows, W D for columns, (W + 1) D and (W - 1) D for the two
+// diagonals), s < 8 and q < W H a pixel index. A box of (D, 8, 1) at (0, 0,
+// q) is the [8][D] tile of the 8 steps of a line from pixel q on, in
+// ascending pixel order: a line going forward (dx > 0 on rows, dy > 0 on the
+// others) has step base + i in row i from the pixel of step base, one going
+// back row 7 - i from the pixel of step base + 7. A copy is only issued for 8
+// steps that all lie on the line, so every byte it reads is the volume's.
+// The maps are encoded on the host for each launch.
+struct CostMaps {
+    CUtensorMap row, column, diagonal, anti;
+};
+
+// Waits of the path scan on its copies that gave up (after kTileWaitNs of
+// the global timer): 0 unless a copy never landed.
+static __device__ unsigned int g_path_wait_failures;
+constexpr uint64_t kTileWaitNs = 1000000000ull;
+#ifndef NXS_TILE_STAGES
+#define NXS_TILE_STAGES 4
+#endif
+constexpr int kTileStages = NXS_TILE_STAGES;  // tiles in flight or read, a line
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned shared_address(const void *p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void barrier_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(shared_address(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void barrier_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void barrier_expect(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(shared_address(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// True once the barrier has completed the phase of `parity`; false when it
+// has not after kTileWaitNs (the clock is read every 256 tries).
+__device__ __forceinline__ bool barrier_wait(uint64_t *bar, unsigned parity) {
+    const unsigned address = shared_address(bar);
+    uint64_t start = 0;
+    for (unsigned i = 0;; ++i) {
+        unsigned done;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            "selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(address), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((i & 255u) == 0) {
+            const uint64_t now = global_ns();
+            if (i == 0) start = now;
+            else if (now - start > kTileWaitNs) return false;
+        }
+    }
+}
+// The tile of a map at (0, 0, pixel) into this CTA's shared memory,
+// completing on `bar` (no multicast: the volume is this GPU's own memory).
+__device__ __forceinline__ void tile_copy(void *to, const CUtensorMap *map, int pixel,
+                                          uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(shared_address(to)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(0), "r"(pixel), "r"(shared_address(bar))
+        : "memory");
+}
+
 // Where the aggregate volume of the summing path scan keeps disparity
 // position j of a pixel (j in the span-16 permuted order of span_disparity,
 // lane j / 16 holding positions 16 * lane ..): the lane's words 0-3 (positions
@@ -504,18 +617,31 @@ __host__ __device__ constexpr int sum_position(int disparities, int j) {
 // patterns: an integer n < 1024 is the f16 subnormal n * 2^-24, and the sum
 // of subnormals below 2^-14 is exact with subnormals kept (.noftz), so the
 // adds are the integer adds (8 directions x at most 127 = 1016).
-template <int G, int WORDS, bool FULL, int THREADS, int SPAN = 0, bool SUMS = false>
+//
+// TILES (8 words a lane, span 16, every lane active): the blocks of 8 steps
+// that every line of the warp covers take their costs from bulk tensor copies
+// (CostMaps) instead of per-lane copies: one lane of each line asks for a
+// block's [8][D] tile kTileStages - 1 blocks ahead into a stage of `tiles`,
+// each stage completing on its own barrier of `bars` (LINES arrivals a
+// phase); the other blocks (each line's last ones) keep the per-lane copies,
+// their ring in the first stage's room once every tile has been read.
+template <int G, int WORDS, bool FULL, int THREADS, int SPAN = 0, bool SUMS = false,
+          bool TILES = false>
 __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
                                              uint8_t *__restrict__ out, const PathSetup &s,
-                                             int p, int line, int member, void *ring_base) {
+                                             int p, int line, int member, void *ring_base,
+                                             const CostMaps *maps = nullptr,
+                                             uint8_t *tiles = nullptr, uint64_t *bars = nullptr) {
     static_assert(WORDS == 4 || WORDS == 8 || WORDS == 16, "4, 8 or 16 words a lane");
     static_assert(SPAN == 0 || (SPAN >= 8 && SPAN <= 2 * WORDS && (2 * WORDS) % SPAN == 0),
                   "a lane holds whole permuted runs");
     static_assert(!SUMS || WORDS == 8, "the aggregate layout has 16 disparities a lane");
+    static_assert(!TILES || (WORDS == 8 && SPAN == 16 && FULL), "tiles of 16 bytes a lane");
     constexpr int BYTES = 2 * WORDS;             // a lane's disparities, one byte each
     constexpr int PIECE = BYTES < 16 ? BYTES : 16;  // bytes of one async copy
     constexpr int PIECES = BYTES / PIECE;
     constexpr int RUN = SPAN / 2;                // words of a permuted run
+    constexpr int LINES = 32 / G;                // lines of a warp
     using Piece = typename std::conditional<PIECE == 16, uint4, uint2>::type;
     Piece *ring = static_cast<Piece *>(ring_base);
     const int dy = s.dy[p], dx = s.dx[p];
@@ -531,12 +657,21 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
     uint8_t *dst = SUMS ? out + 2 * (((size_t)y0 * W + x0) * D + 8 * member)
                         : out + (size_t)p * s.volume + at;
     const int steps = (int)__reduce_max_sync(kFullMask, (unsigned)length);
+    const int shortest = (int)__reduce_min_sync(kFullMask, (unsigned)length);
+    // Blocks all of whose steps every line of the warp has, with the copies they
+    // start (kPrefetch - 1 steps ahead), run without the checks: all blocks of the
+    // rows and columns but the last, most of each diagonal's.
+    auto unchecked_at = [&](int base) { return FULL && base + 2 * kPrefetch - 1 <= shortest; };
 
     uint32_t r[WORDS];
 #pragma unroll
     for (int k = 0; k < WORDS; ++k) r[k] = active ? 0u : kInf2;
     uint32_t m2 = 0, j2 = (uint32_t)s.p2 * 0x10001u;
     const uint32_t p1x2 = (uint32_t)s.p1 * 0x10001u, p2x2 = (uint32_t)s.p2 * 0x10001u;
+    const uint32_t keep_left = member == 0 ? 0u : s.one, edge_left = member == 0 ? kInf2 : 0u;
+    const uint32_t keep_right = member == G - 1 ? 0u : s.one;
+    const uint32_t edge_right = member == G - 1 ? kInf2 : 0u;
+    const uint32_t byte = s.one << 8;  // 256, at run time (pack_run16)
 
     auto fetch = [&](int slot, bool valid) {
 #pragma unroll
@@ -549,11 +684,112 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
         copy_commit();
         ahead = advance(ahead, stride32, s.one);
     };
+    // The ring's first kPrefetch - 1 slots take steps base .. base + kPrefetch - 2.
+    auto prime = [&](int base) {
+        ahead = costs + at + (ptrdiff_t)base * stride;
 #pragma unroll
-    for (int i = 0; i < kPrefetch - 1; ++i) fetch(i, active && i < length);
-    // One block of kPrefetch steps from `base`. CHECKED: the steps test the warp's
-    // last step and each line's end; without, every line of the warp covers the
-    // block and the copies it starts (FULL: every lane active).
+        for (int i = 0; i < kPrefetch - 1; ++i) fetch(i, active && base + i < length);
+    };
+    if (!(TILES && unchecked_at(0))) prime(0);
+
+    // One step from this step's costs: the recurrence on every word, the
+    // store (or reduction) of the path costs where `store`, the line's minimum.
+    auto advance_step = [&](const uint32_t(&cost)[WORDS], bool store) {
+        // The line's first and last lanes see +inf past the ends: x keep + edge
+        // as multiply-adds (keep 0 and edge kInf2 there, 1 and 0 elsewhere).
+        const uint32_t from_left =
+            mad_lo(__shfl_up_sync(kFullMask, r[WORDS - 1], 1), keep_left, edge_left);
+        const uint32_t from_right =
+            mad_lo(__shfl_down_sync(kFullMask, r[0], 1), keep_right, edge_right);
+        const uint32_t negm2 = 0u - m2;
+        uint32_t below[WORDS], above[WORDS];  // word k's values at d - 1 and at d + 1
+        if constexpr (SPAN != 0) {
+#pragma unroll
+            for (int k = 0; k < WORDS; ++k) {
+                const int first = k - k % RUN, last = first + RUN - 1;
+                if (k == first)  // (the run before's last disparity, this run's middle - 1)
+                    below[k] = __byte_perm(first ? r[first - 1] : from_left, r[last], 0x5432);
+                else
+                    below[k] = r[k - 1];
+                if (k == last)  // (this run's middle, the next run's first disparity)
+                    above[k] = __byte_perm(r[first], last + 1 < WORDS ? r[last + 1] : from_right,
+                                           0x5432);
+                else
+                    above[k] = r[k + 1];
+            }
+        } else {
+            uint32_t shifted[WORDS + 1];  // shifted[k]: the (d - 1) values of word k
+            shifted[0] = __byte_perm(from_left, r[0], 0x5432);
+#pragma unroll
+            for (int k = 1; k < WORDS; ++k) shifted[k] = __byte_perm(r[k - 1], r[k], 0x5432);
+            shifted[WORDS] = __byte_perm(r[WORDS - 1], from_right, 0x5432);
+#pragma unroll
+            for (int k = 0; k < WORDS; ++k) {
+                below[k] = shifted[k];
+                above[k] = shifted[k + 1];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < WORDS; ++k) {
+            // min(prev, neighbours + p1, m + p2) - m + cost: neighbours + p1
+            // (a multiply-add by a run-time 1, on the FMA pipe beside the
+            // integer pipe's min and permute work) <= 0x7FFF + 79 stays in its
+            // half; t + cost + (-m) is one three-input add taken mod 2^32,
+            // which equals t - m + cost, whose halves neither borrow nor carry
+            // (t >= m in both). It measured 3% faster than two multiply-adds.
+            const uint32_t neighbour = vmin2(below[k], above[k]);
+            const uint32_t raised = mad_lo(neighbour, s.one, p1x2);
+            const uint32_t t = __vimin3_u16x2(r[k], j2, raised);
+            const uint32_t value = t + cost[k] + negm2;
+            r[k] = (FULL || active) ? value : kInf2;
+        }
+        if (store) {
+            if constexpr (SUMS) {
+                add_sums16(dst, r[0], r[1], r[2], r[3]);
+                add_sums16(dst + D, r[4], r[5], r[6], r[7]);
+            } else {
+#pragma unroll
+                for (int c = 0; c < PIECES; ++c) {
+                    if constexpr (PIECE == 16)
+                        __stcs(reinterpret_cast<uint4 *>(dst + 16 * c),
+                               SPAN ? pack_run16(r + 8 * c, byte) : pack16(r + 8 * c));
+                    else
+                        __stcs(reinterpret_cast<uint2 *>(dst + 8 * c),
+                               SPAN ? pack_run8(r + 4 * c, byte) : pack8(r + 4 * c));
+                }
+            }
+        }
+        dst = advance(dst, SUMS ? 2 * stride32 : stride32, s.one);
+        // The lowest path cost over the line's disparities: a shallow tree
+        // over the lane's words, both halves folded into each half, then
+        // over the line's G lanes a shuffle tree (one warp-wide reduction
+        // when the line has the whole warp; a reduction under each group's
+        // own mask measured slower than the shuffles).
+        constexpr int PARTS = (WORDS + 2) / 3;
+        uint32_t part[PARTS];
+#pragma unroll
+        for (int k = 0; k < WORDS; k += 3)
+            part[k / 3] = k + 2 < WORDS ? __vimin3_u16x2(r[k], r[k + 1], r[k + 2])
+                                        : (k + 1 < WORDS ? vmin2(r[k], r[k + 1]) : r[k]);
+        uint32_t lowest = part[0];
+#pragma unroll
+        for (int k = 1; k < PARTS; k += 2)
+            lowest = k + 1 < PARTS ? __vimin3_u16x2(lowest, part[k], part[k + 1])
+                                   : vmin2(lowest, part[k]);
+        lowest = vmin2(lowest, __byte_perm(lowest, 0, 0x1032));
+        if constexpr (G == 32) {
+            m2 = __reduce_min_sync(kFullMask, lowest);
+        } else {
+#pragma unroll
+            for (int offset = G / 2; offset >= 1; offset /= 2)
+                lowest = vmin2(lowest, __shfl_xor_sync(kFullMask, lowest, offset));
+            m2 = lowest;
+        }
+        j2 = m2 + p2x2;
+    };
+    // One block of kPrefetch steps from `base` from the ring. CHECKED: the steps
+    // test the warp's last step and each line's end; without, every line of the
+    // warp covers the block and the copies it starts (FULL: every lane active).
     auto block = [&](const int base, auto checked) {
         constexpr bool CHECKED = decltype(checked)::value;
 #pragma unroll
@@ -567,110 +803,82 @@ __device__ __forceinline__ void follow_lines(const uint8_t *__restrict__ costs,
             uint32_t cost[WORDS];
 #pragma unroll
             for (int c = 0; c < PIECES; ++c) {
-                if constexpr (PIECE == 16) unpack16(ring[(i * PIECES + c) * THREADS], cost + 8 * c);
-                else unpack8(ring[(i * PIECES + c) * THREADS], cost + 4 * c);
-            }
-            uint32_t from_left = __shfl_up_sync(kFullMask, r[WORDS - 1], 1);
-            uint32_t from_right = __shfl_down_sync(kFullMask, r[0], 1);
-            if (member == 0) from_left = kInf2;
-            if (member == G - 1) from_right = kInf2;
-#ifdef NXS_PATH_IADD3
-            const uint32_t negm2 = 0u - m2;
-#endif
-            uint32_t below[WORDS], above[WORDS];  // word k's values at d - 1 and at d + 1
-            if constexpr (SPAN != 0) {
-#pragma unroll
-                for (int k = 0; k < WORDS; ++k) {
-                    const int first = k - k % RUN, last = first + RUN - 1;
-                    if (k == first)  // (the run before's last disparity, this run's middle - 1)
-                        below[k] = __byte_perm(first ? r[first - 1] : from_left, r[last], 0x5432);
-                    else
-                        below[k] = r[k - 1];
-                    if (k == last)  // (this run's middle, the next run's first disparity)
-                        above[k] = __byte_perm(r[first], last + 1 < WORDS ? r[last + 1] : from_right,
-                                               0x5432);
-                    else
-                        above[k] = r[k + 1];
-                }
-            } else {
-                uint32_t shifted[WORDS + 1];  // shifted[k]: the (d - 1) values of word k
-                shifted[0] = __byte_perm(from_left, r[0], 0x5432);
-#pragma unroll
-                for (int k = 1; k < WORDS; ++k) shifted[k] = __byte_perm(r[k - 1], r[k], 0x5432);
-                shifted[WORDS] = __byte_perm(r[WORDS - 1], from_right, 0x5432);
-#pragma unroll
-                for (int k = 0; k < WORDS; ++k) {
-                    below[k] = shifted[k];
-                    above[k] = shifted[k + 1];
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < WORDS; ++k) {
-                // min(prev, neighbours + p1, m + p2) - m + cost, with the adds on
-                // the FMA pipe (the min and permute work fills the integer pipe):
-                // neighbours + p1 <= 0x7FFF + 79 stays in its half; cost - m is
-                // taken mod 2^32 and t + (cost - m) equals t - m + cost, whose
-                // halves neither borrow nor carry (t >= m in both).
-                const uint32_t neighbour = vmin2(below[k], above[k]);
-                const uint32_t raised = mad_lo(neighbour, s.one, p1x2);
-                const uint32_t t = __vimin3_u16x2(r[k], j2, raised);
-#ifdef NXS_PATH_IADD3
-                const uint32_t value = t + cost[k] + negm2;
-#else
-                const uint32_t value = mad_lo(t, s.one, mad_lo(m2, s.minus_one, cost[k]));
-#endif
-                r[k] = (FULL || active) ? value : kInf2;
-            }
-            if (!CHECKED || (active && step < length)) {
-                if constexpr (SUMS) {
-                    add_sums16(dst, r[0], r[1], r[2], r[3]);
-                    add_sums16(dst + D, r[4], r[5], r[6], r[7]);
+                if constexpr (PIECE == 16) {
+                    if constexpr (SPAN != 0) unpack_run16(ring[(i * PIECES + c) * THREADS], cost + 8 * c);
+                    else unpack16(ring[(i * PIECES + c) * THREADS], cost + 8 * c);
                 } else {
-#pragma unroll
-                    for (int c = 0; c < PIECES; ++c) {
-                        if constexpr (PIECE == 16)
-                            __stcs(reinterpret_cast<uint4 *>(dst + 16 * c), pack16(r + 8 * c));
-                        else
-                            __stcs(reinterpret_cast<uint2 *>(dst + 8 * c), pack8(r + 4 * c));
-                    }
+                    if constexpr (SPAN != 0) unpack_run8(ring[(i * PIECES + c) * THREADS], cost + 4 * c);
+                    else unpack8(ring[(i * PIECES + c) * THREADS], cost + 4 * c);
                 }
             }
-            dst = advance(dst, SUMS ? 2 * stride32 : stride32, s.one);
-            // The lowest path cost over the line's disparities: a shallow tree
-            // over the lane's words, both halves folded into each half, then
-            // over the line's G lanes a shuffle tree (one warp-wide reduction
-            // when the line has the whole warp; a reduction under each group's
-            // own mask measured slower than the shuffles).
-            constexpr int PARTS = (WORDS + 2) / 3;
-            uint32_t part[PARTS];
-#pragma unroll
-            for (int k = 0; k < WORDS; k += 3)
-                part[k / 3] = k + 2 < WORDS ? __vimin3_u16x2(r[k], r[k + 1], r[k + 2])
-                                            : (k + 1 < WORDS ? vmin2(r[k], r[k + 1]) : r[k]);
-            uint32_t lowest = part[0];
-#pragma unroll
-            for (int k = 1; k < PARTS; k += 2)
-                lowest = k + 1 < PARTS ? __vimin3_u16x2(lowest, part[k], part[k + 1])
-                                       : vmin2(lowest, part[k]);
-            lowest = vmin2(lowest, __byte_perm(lowest, 0, 0x1032));
-            if constexpr (G == 32) {
-                m2 = __reduce_min_sync(kFullMask, lowest);
-            } else {
-#pragma unroll
-                for (int offset = G / 2; offset >= 1; offset /= 2)
-                    lowest = vmin2(lowest, __shfl_xor_sync(kFullMask, lowest, offset));
-                m2 = lowest;
-            }
-            j2 = m2 + p2x2;
+            advance_step(cost, !CHECKED || (active && step < length));
         }
     };
-    // Blocks all of whose steps every line of the warp has, with the copies they
-    // start (kPrefetch - 1 steps ahead), run without the checks: all blocks of the
-    // rows and columns but the last, most of each diagonal's.
-    const int shortest = (int)__reduce_min_sync(kFullMask, (unsigned)length);
-    for (int base = 0; base < steps; base += kPrefetch) {
-        if (FULL && base + 2 * kPrefetch - 1 <= shortest) block(base, std::false_type());
-        else block(base, std::true_type());
+
+    if constexpr (TILES) {
+        // Tile rows ascend in pixel index: step base + i is row i going
+        // forward, row 7 - i going back. The unchecked blocks are the first
+        // `tiled` ones; block b's tile is in stage b % kTileStages, asked for
+        // kTileStages - 1 blocks ahead.
+        const bool forward = dy > 0 || (dy == 0 && dx > 0);
+        const int slot_line = (threadIdx.x % 32) / G;
+        const CUtensorMap *map = dy == 0 ? &maps->row
+                                 : dx == 0 ? &maps->column
+                                 : dx == dy ? &maps->diagonal : &maps->anti;
+        const int start = y0 * W + x0, step_pixels = dy * W + dx;  // pixel indices < 2^31
+        const int tiled = shortest >= 2 * kPrefetch - 1 ? (shortest - (2 * kPrefetch - 1)) / kPrefetch + 1 : 0;
+        auto tile_of = [&](int stage) { return tiles + (stage * LINES + slot_line) * kPrefetch * D; };
+        auto issue = [&](int b) {  // block b into its stage
+            if (member == 0) {
+                const int first = forward ? b * kPrefetch : b * kPrefetch + kPrefetch - 1;
+                uint64_t *bar = bars + b % kTileStages;
+                barrier_expect(bar, (unsigned)(kPrefetch * D));
+                tile_copy(tile_of(b % kTileStages), map, start + first * step_pixels, bar);
+            }
+        };
+        auto wait_block = [&](int b) {
+            return barrier_wait(bars + b % kTileStages, (unsigned)(b / kTileStages) & 1u);
+        };
+        for (int b = 0; b < tiled && b < kTileStages - 1; ++b) issue(b);
+        for (int b = 0; b < tiled; ++b) {
+            __syncwarp();  // every lane has read block b - 1's stage
+            if (b + kTileStages - 1 < tiled) issue(b + kTileStages - 1);
+            if (!__all_sync(kFullMask, wait_block(b))) {
+                // A copy that never landed: count it, give the others in
+                // flight the same time, and leave this warp's lines unfinished.
+                if ((threadIdx.x % 32) == 0) atomicAdd(&g_path_wait_failures, 1u);
+                for (int k = b + 1; k < tiled && k < b + kTileStages; ++k) wait_block(k);
+                return;
+            }
+            const uint4 *tile = reinterpret_cast<const uint4 *>(tile_of(b % kTileStages)) + member;
+            if (forward) {
+#pragma unroll
+                for (int i = 0; i < kPrefetch; ++i) {
+                    uint32_t cost[WORDS];
+                    unpack_run16(tile[i * G], cost);
+                    advance_step(cost, true);
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < kPrefetch; ++i) {
+                    uint32_t cost[WORDS];
+                    unpack_run16(tile[(kPrefetch - 1 - i) * G], cost);
+                    advance_step(cost, true);
+                }
+            }
+        }
+        // The rest from the ring, which shares the first stage's room: every
+        // tile has landed and been read (the barrier below) before it refills.
+        __syncwarp();
+        for (int base = tiled * kPrefetch; base < steps; base += kPrefetch) {
+            if (base == tiled * kPrefetch && tiled > 0) prime(base);
+            block(base, std::true_type());
+        }
+    } else {
+        for (int base = 0; base < steps; base += kPrefetch) {
+            if (unchecked_at(base)) block(base, std::false_type());
+            else block(base, std::true_type());
+        }
     }
     copy_wait<0>();
 }
@@ -704,10 +912,12 @@ __host__ __device__ __forceinline__ int ranked_line(int rank, int dy, int dx, in
 // Rows, then columns, then the diagonals of all four directions by rank.
 // `ring`: this lane's first slot of the warp's kPrefetch x 32 slots of
 // 2 x WORDS bytes (in pieces of at most 16 bytes, strided by 32 lanes).
-template <int G, int WORDS, bool FULL, int SPAN = 0, bool SUMS = false>
+template <int G, int WORDS, bool FULL, int SPAN = 0, bool SUMS = false, bool TILES = false>
 __device__ __forceinline__ void path_warp(const uint8_t *__restrict__ costs,
                                           uint8_t *__restrict__ paths_out, const PathSetup &s,
-                                          int warp, int lane, void *ring) {
+                                          int warp, int lane, void *ring,
+                                          const CostMaps *maps = nullptr, uint8_t *tiles = nullptr,
+                                          uint64_t *bars = nullptr) {
     int slot = 0;
     while (warp >= s.first_warp[slot + 1]) ++slot;
     int p, group;
@@ -723,7 +933,8 @@ __device__ __forceinline__ void path_warp(const uint8_t *__restrict__ costs,
     const int rank = group * (32 / G) + lane / G;
     const int line =
         rank < s.lines[p] ? ranked_line(rank, s.dy[p], s.dx[p], s.width, s.height) : rank;
-    follow_lines<G, WORDS, FULL, 32, SPAN, SUMS>(costs, paths_out, s, p, line, lane % G, ring);
+    follow_lines<G, WORDS, FULL, 32, SPAN, SUMS, TILES>(costs, paths_out, s, p, line, lane % G,
+                                                        ring, maps, tiles, bars);
 }
 
 // Lanes per pixel (selection) or per line (paths with 16 disparities a lane),
@@ -741,6 +952,18 @@ __host__ __device__ inline int path_lanes(int disparities, int words) {
 }
 
 // ---------------------------------------------------------------- select
+// Which disparity half h of word k of a selection lane's 16 holds (j = 2k +
+// h): the volumes' bytes 2k and 2k + 1 (span_disparity), or for the summing
+// scan's aggregate (PATHS -1) the scan lane's word k, (k, k + 8); and where
+// disparity d lies in the per-pixel row of 16-value runs.
+template <int PATHS, int SPAN>
+__host__ __device__ constexpr int select_disparity(int j) {
+    return PATHS == -1 ? (j % 16) / 2 + 8 * (j % 2) + 16 * (j / 16) : span_disparity(SPAN, j);
+}
+template <int PATHS, int SPAN>
+__host__ __device__ constexpr int select_position(int d) {
+    return PATHS == -1 ? 16 * (d / 16) + 2 * (d % 8) + (d % 16) / 8 : span_position(SPAN, d);
+}
 // Winner, uniqueness and subpixel (lib/nx_stereo.ex:608-641). A group of G
 // lanes takes one pixel, each lane 16 disparities, so a warp takes 32 / G
 // pixels. values = sum of the path costs + 0x8000 past x; the winner is the
@@ -814,8 +1037,8 @@ __device__ __forceinline__ void select_pixels(const void *__restrict__ source, i
         if (x < d0 + 15) {  // disparities past the left edge lose
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
-                const int lo = d0 + span_disparity(SPAN, 2 * k);
-                const int hi = d0 + span_disparity(SPAN, 2 * k + 1);
+                const int lo = d0 + select_disparity<PATHS, SPAN>(2 * k);
+                const int hi = d0 + select_disparity<PATHS, SPAN>(2 * k + 1);
                 v[k] += (lo > x ? 0x8000u : 0u) | (hi > x ? 0x80000000u : 0u);
             }
         }
@@ -826,8 +1049,8 @@ __device__ __forceinline__ void select_pixels(const void *__restrict__ source, i
     if (active) {
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const uint32_t lo = d0 + span_disparity(SPAN, 2 * k);
-            const uint32_t hi = d0 + span_disparity(SPAN, 2 * k + 1);
+            const uint32_t lo = d0 + select_disparity<PATHS, SPAN>(2 * k);
+            const uint32_t hi = d0 + select_disparity<PATHS, SPAN>(2 * k + 1);
             const uint32_t d = lo | (hi << 16);
             best = min(best, min(__byte_perm(v[k], d, 0x1054), __byte_perm(v[k], d, 0x3276)));
         }
@@ -841,8 +1064,8 @@ __device__ __forceinline__ void select_pixels(const void *__restrict__ source, i
     if (active) {
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const int lo = d0 + span_disparity(SPAN, 2 * k);
-            const int hi = d0 + span_disparity(SPAN, 2 * k + 1);
+            const int lo = d0 + select_disparity<PATHS, SPAN>(2 * k);
+            const int hi = d0 + select_disparity<PATHS, SPAN>(2 * k + 1);
             // d outside [winner - 1, winner + 1]
             if ((unsigned)(lo - winner + 1) > 2u) second = min(second, v[k] & 0xFFFFu);
             if ((unsigned)(hi - winner + 1) > 2u) second = min(second, v[k] >> 16);
@@ -854,8 +1077,8 @@ __device__ __forceinline__ void select_pixels(const void *__restrict__ source, i
     __syncwarp();
     if (member != 0 || !valid) return;
     const int below = max(winner - 1, 0), above = min(winner + 1, D - 1);
-    const uint32_t lower = values_of[slot][span_position(SPAN, below)];
-    const uint32_t upper = values_of[slot][span_position(SPAN, above)];
+    const uint32_t lower = values_of[slot][select_position<PATHS, SPAN>(below)];
+    const uint32_t upper = values_of[slot][select_position<PATHS, SPAN>(above)];
     const float lower_f = (float)lower, upper_f = (float)upper, minimum_f = (float)minimum;
     // With no disparity outside the winner's neighbours the reference's
     // minimum is i32::MAX (lib/nx_stereo.ex:620-622).

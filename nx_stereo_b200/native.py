@@ -129,6 +129,9 @@ SIGNATURES = {
     "nxs_path_words": (_u32, [_u32]),
     "nxs_set_path_sums": (_i, [_u32]),
     "nxs_path_sums": (_u32, [_u32, _u32, _u32]),
+    "nxs_set_path_tiles": (_i, [_u32]),
+    "nxs_path_tiles": (_u32, []),
+    "nxs_path_wait_failures": (_u32, []),
     "nxs_band_check": (_i, [ctypes.POINTER(BandParams), _u32, _u32, ctypes.c_int32] + _err),
     "nxs_band_scratch_bytes": (_u64, [_u32, _u32, _u32, ctypes.c_int32]),
     "nxs_sgm_band_device": (_i, [_P, _P, _P, _P, _u32, _u32, ctypes.POINTER(BandParams), _P, _P]

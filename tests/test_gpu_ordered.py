@@ -1,8 +1,10 @@
 """The matcher's internal disparity order: the _ordered entry points write and
 read the same values as the natural-order ones (which the oracle pins), each
-run of `span` disparities permuted so that bytes 2k and 2k + 1 hold
-disparities k and k + span / 2; selection from ordered volumes equals
-selection from natural ones bit for bit."""
+run of `span` disparities permuted so that bytes 4q .. 4q + 3 hold
+disparities 2q, 2q + 1, 2q + span / 2 and 2q + 1 + span / 2 (a path lane's
+words 2q and 2q + 1, each word k holding k and k + span / 2, interleaved);
+selection from ordered volumes equals selection from natural ones bit for
+bit."""
 import numpy as np
 import pytest
 
@@ -20,7 +22,8 @@ def position(d, span):
     if span == 0:
         return d
     half = span // 2
-    return (d // span) * span + 2 * ((d % span) % half) + (d % span) // half
+    within = d % span
+    return (d // span) * span + 4 * ((within % half) // 2) + d % 2 + 2 * (within // half)
 
 
 def permuted(volume, span):
@@ -34,7 +37,9 @@ def test_position_is_a_permutation_and_pairs_neighbours():
         p = position(np.arange(64), span)
         assert sorted(p.tolist()) == list(range(64))
         inverse = np.argsort(p)  # byte j of a run holds disparity inverse[j]
-        assert inverse[:span].tolist() == [k // 2 + (span // 2) * (k % 2) for k in range(span)]
+        # bytes 4q .. 4q + 3: words 2q and 2q + 1 interleaved, word k = (k, k + span / 2)
+        assert inverse[:span].tolist() == [2 * (j // 4) + j % 2 + (span // 2) * ((j // 2) % 2)
+                                           for j in range(span)]
 
 
 @pytest.fixture(scope="module")
