@@ -50,7 +50,7 @@ PATHS_EVERY = 4  # timed steps between those whose path kernel is bracketed by e
 SERVING_CAP = None
 # DRAM bytes (read + write) of one path-aggregation launch on this workload, from
 # an ncu capture of this command (dram__bytes_read.sum + dram__bytes_write.sum).
-PATHS_TRAFFIC_BYTES = 107_285_504 + 350_222_336
+PATHS_TRAFFIC_BYTES = 111_123_200 + 349_851_392
 
 
 # The workload's config, the same on both arms.
@@ -387,8 +387,9 @@ def run_ours(args, rank, world, local_rank):
                      "algorithmic_bytes_per_launch": paths_bytes,
                      "avg_launch_ms": round(paths_avg_s * 1000, 4),
                      "traffic": PATHS_TRAFFIC_BYTES,
-                     "limiter": "instruction issue of the scan-line steps with ~8 warps a SM "
-                                "(ncu: issue 59%, integer ALU pipe 55%, FMA pipe 17%, HBM 43%)"},
+                     "limiter": "dependent latency of the longest scan lines' steps and "
+                                "instruction issue with ~8 warps a SM (ncu: issue 55%, integer "
+                                "ALU pipe 59%, FMA pipe 12%, HBM 44%)"},
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "stages_ms_from": "a second run of the same steps with an event between every stage",
         "pipeline_roofline": {"b_alg_per_pair": b_alg,
