@@ -836,6 +836,18 @@ def run_reference(args):
                     "d2h_bytes_per_step": 0}}
 
 
+def section(name, run):
+    """One of the bench's sections inside an NVTX range of its name, so that a
+    profiler can take its launches alone (ncu --nvtx --nvtx-include name/)."""
+    import torch
+
+    torch.cuda.nvtx.range_push(name)
+    try:
+        return run()
+    finally:
+        torch.cuda.nvtx.range_pop()
+
+
 def main():
     from nx_stereo_b200 import replicas
 
@@ -859,16 +871,16 @@ def main():
 
         ctx = native.Context(local_rank)
         if not args.no_batch:
-            line["batched"] = bench_batched(torch, ctx)
+            line["batched"] = section("batched", lambda: bench_batched(torch, ctx))
         if not args.no_large:
-            line["large_range"] = bench_large(torch, ctx)
+            line["large_range"] = section("large_range", lambda: bench_large(torch, ctx))
         if not args.no_coarse_to_fine:
-            line["coarse_to_fine"] = bench_coarse_to_fine(torch, ctx)
+            line["coarse_to_fine"] = section("coarse_to_fine", lambda: bench_coarse_to_fine(torch, ctx))
         if not args.no_cpu_baseline:
-            line["config0"] = bench_config0(torch, ctx)
+            line["config0"] = section("config0", lambda: bench_config0(torch, ctx))
         ctx.close()
         if not args.no_serving:
-            line["serving"] = bench_serving()
+            line["serving"] = section("serving", lambda: bench_serving())
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
         rig, frames = make_inputs(4, seed=1)
