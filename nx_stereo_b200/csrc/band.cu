@@ -277,10 +277,7 @@ __global__ void __launch_bounds__(32)
 #pragma unroll
         for (int k = 1; k < WORDS; ++k) lowest = vmin2(lowest, r[k]);
         lowest = vmin2(lowest, __byte_perm(lowest, 0, 0x1032));
-#pragma unroll
-        for (int offset = G / 2; offset >= 1; offset /= 2)
-            lowest = vmin2(lowest, __shfl_xor_sync(kFullMask, lowest, offset));
-        m2 = lowest;
+        m2 = line_minimum<G>(lowest);
         __syncwarp();  // every lane has read the row
 #pragma unroll
         for (int k = 0; k < WORDS; ++k) row[(Row::PAD + member * V) / 2 + k] = r[k] - m2;
