@@ -5,6 +5,8 @@ no CPU fallback, and loading fails loudly when it is missing or cannot open a
 CUDA device.
 """
 import ctypes
+import struct
+import threading
 import os
 
 import numpy as np
@@ -214,8 +216,16 @@ def _check(status, buf):
         raise NativeError(status, buf.value.decode("utf-8", "replace") if buf is not None else "")
 
 
+_local = threading.local()
+
+
 def _errbuf():
-    return ctypes.create_string_buffer(1024)
+    """This thread's error-text buffer (each call reads it before the next)."""
+    buf = getattr(_local, "errbuf", None)
+    if buf is None:
+        buf = _local.errbuf = ctypes.create_string_buffer(1024)
+    buf[0] = b"\0"
+    return buf
 
 
 def sgm_params(disparities=64, paths=8, p1=8, p2=64, uniqueness=1.0526315789473684,
@@ -251,6 +261,12 @@ def make_camera(k, d, inverse_pr):
     cam.d[:] = [float(v) for v in np.asarray(d, np.float32).ravel()]
     cam.inverse_pr[:] = [float(v) for v in np.asarray(inverse_pr, np.float32).ravel()]
     return cam
+
+
+# nxs_tensor as laid out in memory: name, type, rank, dims[4], data, bytes.
+_TENSOR = struct.Struct("<QII4IQQ")
+assert _TENSOR.size == ctypes.sizeof(Tensor)
+_LAYOUTS = {}  # output descriptors without their addresses -> (name, dtype, shape, bytes)
 
 
 class _PinnedView:
@@ -313,12 +329,28 @@ class Request:
         tensors = ctypes.POINTER(Tensor)()
         _check(load().nxs_request_outputs(self._handle, ctypes.byref(n), ctypes.byref(tensors)),
                None)
+        if n.value == 0:
+            return {}
+        # The descriptors in one read; their names, types and shapes are the
+        # segment's, so their layout is worked out once and kept.
+        raw = ctypes.string_at(ctypes.addressof(tensors.contents), n.value * _TENSOR.size)
+        fields = list(_TENSOR.iter_unpack(raw))
+        key = tuple(f[:7] + f[8:] for f in fields)
+        layout = _LAYOUTS.get(key)
+        if layout is None:
+            layout = [(ctypes.string_at(f[0]).decode(), np.dtype(DTYPES[f[1]]), tuple(f[3:3 + f[2]]),
+                       f[8]) for f in fields]
+            _LAYOUTS[key] = layout
+        # One view spanning the outputs (one pinned block when they are packed),
+        # each output a slice of it.
+        datas = [f[7] for f in fields]
+        low = min(datas)
+        high = max(d + entry[3] for d, entry in zip(datas, layout))
+        block = np.asarray(_PinnedView(self, low, (high - low,), np.dtype(np.uint8)))
         result = {}
-        for i in range(n.value):
-            t = tensors[i]
-            shape = tuple(t.dims[:t.rank])
-            view = np.asarray(_PinnedView(self, t.data, shape, np.dtype(DTYPES[t.type])))
-            result[t.name.decode()] = view.copy() if copy else view
+        for d, (name, dtype, shape, nbytes) in zip(datas, layout):
+            view = block[d - low:d - low + nbytes].view(dtype).reshape(shape)
+            result[name] = view.copy() if copy else view
         return result
 
     def done_ns(self):
@@ -402,13 +434,26 @@ class Context:
         if not isinstance(params, PreparedParams):
             params = PreparedParams(params)
         mps, keep = params.members, [params]
-        ts = (Tensor * max(len(entries), 1))()
-        for i, (name, array) in enumerate(entries.items()):
-            a = np.ascontiguousarray(array)
-            b = name.encode()
-            keep += [b, a]
-            dims = (ctypes.c_uint32 * 4)(*(list(a.shape) + [0] * (4 - a.ndim)))
-            ts[i] = Tensor(b, TYPE_CODES[a.dtype], a.ndim, dims, a.ctypes.data, a.nbytes)
+        arrays = [np.ascontiguousarray(a) for a in entries.values()]
+        # The descriptors of entries of these names, types and shapes are made
+        # once a thread and reused with the new addresses (the call copies the
+        # entries before it returns).
+        key = tuple((name, a.dtype.str, a.shape) for name, a in zip(entries, arrays))
+        cache = getattr(_local, "entries", None)
+        if cache is None:
+            cache = _local.entries = {}
+        ts = cache.get(key)
+        if ts is None:
+            ts = (Tensor * max(len(arrays), 1))()
+            names = [name.encode() for name in entries]
+            for i, (b, a) in enumerate(zip(names, arrays)):
+                dims = (ctypes.c_uint32 * 4)(*(list(a.shape) + [0] * (4 - a.ndim)))
+                ts[i] = Tensor(b, TYPE_CODES[a.dtype], a.ndim, dims, 0, a.nbytes)
+            ts._names = names  # the descriptors point at these bytes
+            cache[key] = ts
+        for i, a in enumerate(arrays):
+            ts[i].data = a.ctypes.data
+        keep.append(arrays)
         callback = DONE_FN(done) if done else DONE_FN()
         handle = ctypes.c_void_p()
         buf = _errbuf()
