@@ -50,7 +50,7 @@ PATHS_EVERY = 4  # timed steps between those whose path kernel is bracketed by e
 SERVING_CAP = None
 # DRAM bytes (read + write) of one path-aggregation launch on this workload, from
 # an ncu capture of this command (dram__bytes_read.sum + dram__bytes_write.sum).
-PATHS_TRAFFIC_BYTES = 111_123_200 + 349_851_392
+PATHS_TRAFFIC_BYTES = 114_332_416 + 350_151_936
 
 
 # The workload's config, the same on both arms.
@@ -388,8 +388,8 @@ def run_ours(args, rank, world, local_rank):
                      "avg_launch_ms": round(paths_avg_s * 1000, 4),
                      "traffic": PATHS_TRAFFIC_BYTES,
                      "limiter": "dependent latency of the longest scan lines' steps and "
-                                "instruction issue with ~8 warps a SM (ncu: issue 55%, integer "
-                                "ALU pipe 59%, FMA pipe 12%, HBM 44%)"},
+                                "instruction issue with ~8 warps a SM (ncu: issue 57%, integer "
+                                "ALU pipe 61%, FMA pipe 12%, HBM 45%)"},
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "stages_ms_from": "a second run of the same steps with an event between every stage",
         "pipeline_roofline": {"b_alg_per_pair": b_alg,
