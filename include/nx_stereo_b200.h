@@ -220,6 +220,15 @@ uint32_t nxs_path_sums(uint32_t width, uint32_t height, uint32_t disparities);
  * on the current device (each wait is bounded, about 1 s; 0 unless a copy
  * never landed, after which that launch's path volumes are incomplete). */
 nxs_status nxs_set_path_tiles(uint32_t mode);
+
+/* Segments configured after the call (on 1, the default) run a full-search
+ * Disparity member split over two streams when none of their stages carries
+ * state: each pair's census, costs and path volumes on one, its selection
+ * onwards on the other, so that one pair's path scan runs beside the pair
+ * before's selection; pairs alternate between two matcher scratches. Off (0):
+ * each pair runs wholly on one of two streams, pairs alternating. Results do
+ * not depend on it. */
+nxs_status nxs_set_split_lanes(uint32_t on);
 uint32_t nxs_path_tiles(void);
 uint32_t nxs_path_wait_failures(void);
 

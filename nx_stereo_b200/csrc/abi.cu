@@ -261,6 +261,9 @@ struct Slot {
 // order on one stream.
 constexpr int kSlots = 4;
 constexpr int kLanes = 2;
+// Whether segments configured from now on split their matcher over two
+// streams (Segment::split); set by nxs_set_split_lanes.
+static bool g_split_lanes = true;
 
 struct Segment {
     uint32_t id = 0;
@@ -292,6 +295,14 @@ struct Segment {
     // shared by the requests of one compute lane, touched only on its stream
     float *depth_m[kLanes] = {}, *quality_columns = nullptr;
     DeviceBuffer scratch[kLanes];
+    // Split: a segment without carried state whose Disparity member is the
+    // full search runs each pair's census, costs and path volumes on lanes[0]
+    // and its selection onwards on lanes[1], so pair n + 1's path scan (bound
+    // by its steps' latency and the integer pipe) runs beside pair n's
+    // selection (bound by HBM). Requests alternate between the two scratches;
+    // carved[k]: scratch k's path volumes written, freed[k]: read.
+    bool split = false;
+    cudaEvent_t carved[kLanes] = {}, freed[kLanes] = {};
     std::vector<void *> allocations;
 
     std::vector<cudaStream_t> streams() const {
@@ -318,6 +329,9 @@ struct Segment {
         for (DeviceBuffer &b : scratch) b.release();
         for (Slot &slot : slots)
             for (cudaEvent_t ev : {slot.entered, slot.free})
+                if (ev) cudaEventDestroy(ev);
+        for (int k = 0; k < kLanes; ++k)
+            for (cudaEvent_t ev : {carved[k], freed[k]})
                 if (ev) cudaEventDestroy(ev);
         for (cudaStream_t st : streams())
             if (st) cudaStreamDestroy(st);
@@ -455,6 +469,12 @@ extern "C" nxs_status nxs_set_path_sums(uint32_t mode) {
 
 extern "C" uint32_t nxs_path_sums(uint32_t width, uint32_t height, uint32_t disparities) {
     return path_sums_wanted((int)width, (int)height, (int)disparities) ? 1u : 0u;
+}
+
+extern "C" nxs_status nxs_set_split_lanes(uint32_t on) {
+    if (on > 1) return NXS_BAD_ARGUMENT;
+    g_split_lanes = on != 0;
+    return NXS_OK;
 }
 
 extern "C" nxs_status nxs_set_path_tiles(uint32_t mode) {
@@ -1353,6 +1373,9 @@ extern "C" nxs_status nxs_configure(nxs_context *c, uint32_t id, const nxs_geome
     for (const Member &m : seg->members)
         carries = carries || m.kind == Kind::Temporal || m.kind == Kind::Quality;
     seg->n_lanes = carries ? 1 : kLanes;
+    for (const Member &m : seg->members)
+        if (m.kind == Kind::Disparity && !m.coarse_to_fine && seg->n_lanes == 2 && g_split_lanes)
+            seg->split = true;
     for (cudaStream_t *st : {&seg->upload, &seg->download, &seg->notify})
         if (!e) e = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
     for (int k = 0; k < seg->n_lanes; ++k)
@@ -1446,6 +1469,8 @@ extern "C" nxs_status nxs_configure(nxs_context *c, uint32_t id, const nxs_geome
     for (int k = 0; k < seg->n_lanes; ++k) {
         if (!e) e = seg->alloc(&seg->depth_m[k], pixels);
         if (!e && max_disparities) e = seg->scratch[k].reserve(matcher_scratch);
+        for (cudaEvent_t *ev : {&seg->carved[k], &seg->freed[k]})
+            if (!e && seg->split) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
     }
     if (!e) e = seg->alloc(&seg->quality_columns, 5 * (size_t)g.width);
     // What the stages carry starts over: previous = -1, missed = 0
@@ -1587,8 +1612,10 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
     std::lock_guard<std::mutex> order(seg->order);
     const uint64_t sequence = seg->sequence++;
     Slot &slot = seg->slots[sequence % kSlots];
+    // Split segments: `lane` picks the scratch and depth map; the pair starts
+    // on lanes[0] and moves to lanes[1] after its path volumes.
     const int lane = (int)(sequence % (uint64_t)seg->n_lanes);
-    cudaStream_t s = seg->lanes[lane];
+    cudaStream_t s = seg->lanes[seg->split ? 0 : lane];
     const size_t pixels = (size_t)g.width * g.height;
     // Upload, once the slot's last request has downloaded its outputs.
     e = cudaStreamWaitEvent(seg->upload, slot.free, 0);
@@ -1620,9 +1647,26 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
             }
             MatcherScratch ms =
                 carve_matcher_scratch(seg->scratch[lane].ptr, g.width, g.height, m.disparities);
-            e = run_matcher(slot.images[0], slot.images[1], g.width, g.height, m.disparities,
-                            m.paths, l.sgm.p1, l.sgm.p2, l.sgm.uniqueness, 1, ms,
-                            slot.disparity[current], s);
+            if (!seg->split) {
+                e = run_matcher(slot.images[0], slot.images[1], g.width, g.height, m.disparities,
+                                m.paths, l.sgm.p1, l.sgm.p2, l.sgm.uniqueness, 1, ms,
+                                slot.disparity[current], s);
+                break;
+            }
+            // The front half once the pair two before has read this scratch (an
+            // event not yet recorded is no wait); the rest on the back stream.
+            cudaStream_t back = seg->lanes[1];
+            e = cudaStreamWaitEvent(s, seg->freed[lane], 0);
+            if (!e)
+                e = run_matcher_front(slot.images[0], slot.images[1], g.width, g.height,
+                                      m.disparities, m.paths, l.sgm.p1, l.sgm.p2, ms, s);
+            if (!e) e = cudaEventRecord(seg->carved[lane], s);
+            if (!e) e = cudaStreamWaitEvent(back, seg->carved[lane], 0);
+            if (!e)
+                e = run_matcher_back(g.width, g.height, m.disparities, m.paths,
+                                     l.sgm.uniqueness, 1, ms, slot.disparity[current], back);
+            if (!e) e = cudaEventRecord(seg->freed[lane], back);
+            s = back;
             break;
         }
         case Kind::Speckle:

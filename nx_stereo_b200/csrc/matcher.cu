@@ -616,34 +616,45 @@ MatcherScratch carve_matcher_scratch(void *base, int width, int height, int disp
     return s;
 }
 
-cudaError_t run_matcher(const uint8_t *left, const uint8_t *right, int width, int height,
-                        int disparities, int paths, int p1, int p2, float uniqueness,
-                        int stage_mask, const MatcherScratch &s, float *disparity,
-                        cudaStream_t stream) {
+cudaError_t run_matcher_front(const uint8_t *left, const uint8_t *right, int width, int height,
+                              int disparities, int paths, int p1, int p2,
+                              const MatcherScratch &s, cudaStream_t stream) {
     cudaError_t e;
     // The intermediates are in the permuted order of the path lanes' span
     // (span_disparity).
     const int span = matcher_span(disparities);
     if ((e = launch_census_costs(left, right, width, height, disparities, s.costs, stream, span)))
         return e;
-    if (path_sums_wanted(width, height, disparities)) {  // the aggregate in the path volumes' room
-        uint16_t *sums = reinterpret_cast<uint16_t *>(s.paths);
-        if ((e = launch_paths_sums(s.costs, width, height, disparities, paths, p1, p2, sums,
-                                   stream)))
-            return e;
-        if ((e = launch_select_path_sums(sums, width, height, disparities, uniqueness,
-                                         s.selected, s.keys, stream)))
-            return e;
-        return launch_check_median(s.selected, s.keys, width, height, stage_mask, disparity,
-                                   stream);
-    }
-    if ((e = launch_paths(s.costs, width, height, disparities, paths, p1, p2, s.paths, stream,
-                          span)))
-        return e;
-    if ((e = launch_select_paths(s.paths, width, height, disparities, paths, uniqueness,
-                                 s.selected, s.keys, stream, span)))
-        return e;
+    if (path_sums_wanted(width, height, disparities))  // the aggregate in the path volumes' room
+        return launch_paths_sums(s.costs, width, height, disparities, paths, p1, p2,
+                                 reinterpret_cast<uint16_t *>(s.paths), stream);
+    return launch_paths(s.costs, width, height, disparities, paths, p1, p2, s.paths, stream,
+                        span);
+}
+
+cudaError_t run_matcher_back(int width, int height, int disparities, int paths,
+                             float uniqueness, int stage_mask, const MatcherScratch &s,
+                             float *disparity, cudaStream_t stream) {
+    cudaError_t e;
+    if (path_sums_wanted(width, height, disparities))
+        e = launch_select_path_sums(reinterpret_cast<const uint16_t *>(s.paths), width, height,
+                                    disparities, uniqueness, s.selected, s.keys, stream);
+    else
+        e = launch_select_paths(s.paths, width, height, disparities, paths, uniqueness,
+                                s.selected, s.keys, stream, matcher_span(disparities));
+    if (e) return e;
     return launch_check_median(s.selected, s.keys, width, height, stage_mask, disparity, stream);
+}
+
+cudaError_t run_matcher(const uint8_t *left, const uint8_t *right, int width, int height,
+                        int disparities, int paths, int p1, int p2, float uniqueness,
+                        int stage_mask, const MatcherScratch &s, float *disparity,
+                        cudaStream_t stream) {
+    const cudaError_t e =
+        run_matcher_front(left, right, width, height, disparities, paths, p1, p2, s, stream);
+    if (e) return e;
+    return run_matcher_back(width, height, disparities, paths, uniqueness, stage_mask, s,
+                            disparity, stream);
 }
 
 }  // namespace nxs

@@ -132,6 +132,15 @@ cudaError_t run_matcher(const uint8_t *left, const uint8_t *right, int width, in
                         int disparities, int paths, int p1, int p2, float uniqueness,
                         int stage_mask, const MatcherScratch &scratch, float *disparity,
                         cudaStream_t stream);
+// Its two halves: the census, costs and path volumes (front); selection, the
+// check and the median from the path volumes (back). run_matcher runs both on
+// one stream; a segment may run them on two, pairs apart.
+cudaError_t run_matcher_front(const uint8_t *left, const uint8_t *right, int width, int height,
+                              int disparities, int paths, int p1, int p2,
+                              const MatcherScratch &scratch, cudaStream_t stream);
+cudaError_t run_matcher_back(int width, int height, int disparities, int paths,
+                             float uniqueness, int stage_mask, const MatcherScratch &scratch,
+                             float *disparity, cudaStream_t stream);
 
 // ---- the coarse-to-fine search (band.cu) ----
 // Both images' rounded 2x2 means.

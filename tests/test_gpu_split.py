@@ -1,0 +1,68 @@
+"""A segment whose matcher runs split over two streams (each pair's census,
+costs and path volumes on one, its selection onwards on the other, pairs
+alternating between two scratches) gives every pair the same outputs as the
+unsplit segment and as the oracle, with many pairs in flight."""
+import numpy as np
+import pytest
+
+from tests import gpu_util as g
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(split, pairs, frames_of, w, h):
+    from nx_stereo_b200 import native, segment, stage
+
+    native.load().nxs_set_split_lanes(1 if split else 0)
+    try:
+        geometry = segment.standard_geometry(w, h)
+        status, members = segment.members(
+            [stage.Rectification, (stage.Disparity, {"num_disparities": 128}),
+             stage.SpeckleFilter, stage.Depth, (stage.PointCloud, {"decimation": 4})], geometry)
+        assert status == "ok", members
+        status, seg = segment.CudaSegment.build(members, geometry)
+        assert status == "ok", seg
+        sent = []
+        for k in range(pairs):  # all sent before any is awaited
+            status, request = segment.CudaSegment.send_request(frames_of(k), seg)
+            assert status == "ok"
+            sent.append(request)
+        replies = []
+        for request in sent:
+            reply = segment.CudaSegment.await_(request, seg, 60000)
+            assert reply[0] == "ok", reply
+            replies.append({k: np.array(v) for k, v in reply[1].items()})
+        seg.release()
+        return replies
+    finally:
+        native.load().nxs_set_split_lanes(1)
+
+
+def test_split_equals_unsplit_and_the_oracle(oracle):
+    from nx_stereo_b200 import scene, segment
+
+    w, h = 728, 544
+    rig = scene.rig(w, h)
+    frames = []
+    for k in range(6):
+        left, right = scene.rectified_pair(w, h, seed=90 + k, rectangles=6, max_disparity=120)
+        frames.append(scene.raw_frames(left, right, rig))
+
+    def frames_of(k):
+        return {"left_frame": frames[k % 6][0], "right_frame": frames[k % 6][1]}
+
+    split = _run(True, 9, frames_of, w, h)
+    plain = _run(False, 9, frames_of, w, h)
+    for a, b in zip(split, plain):
+        assert a.keys() == b.keys()
+        for key in a:
+            assert a[key].tobytes() == b[key].tobytes(), key
+    # the first pair against the oracle's chain
+    geometry = segment.standard_geometry(w, h)
+    cams = [geometry["left_camera"], geometry["right_camera"]]
+    images = [oracle.rectify(f, oracle.make_camera(c["k"], c["d"], c["inverse_pr"]), (h, w))
+              for f, c in zip(frames[0], cams)]
+    d = oracle.fast_sgm(images[0], images[1], 128, 8)
+    d = np.where(d > 0, d, np.float32(-1.0)).astype(np.float32)
+    want = oracle.despeckle(d, 12, 1.0, 3)
+    assert g.same_bits(split[0]["disparity"], want)
