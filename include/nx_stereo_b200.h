@@ -222,11 +222,13 @@ uint32_t nxs_path_sums(uint32_t width, uint32_t height, uint32_t disparities);
 nxs_status nxs_set_path_tiles(uint32_t mode);
 
 /* Segments configured after the call (on 1, the default) run a full-search
- * Disparity member split over two streams when none of their stages carries
- * state: each pair's census, costs and path volumes on one, its selection
- * onwards on the other, so that one pair's path scan runs beside the pair
- * before's selection; pairs alternate between two matcher scratches. Off (0):
- * each pair runs wholly on one of two streams, pairs alternating. Results do
+ * Disparity member split over two streams when no stage before it carries
+ * state: each pair's stages up to its census, costs and path volumes on one,
+ * its selection and the stages after (TemporalFilter and Quality among them,
+ * in request order) on the other, so that one pair's front half runs beside
+ * the pair before's back half; pairs alternate between two matcher scratches.
+ * Off (0): a segment without state runs each pair wholly on one of two
+ * streams, pairs alternating, and one with state on one stream. Results do
  * not depend on it. */
 nxs_status nxs_set_split_lanes(uint32_t on);
 uint32_t nxs_path_tiles(void);

@@ -295,12 +295,12 @@ struct Segment {
     // shared by the requests of one compute lane, touched only on its stream
     float *depth_m[kLanes] = {}, *quality_columns = nullptr;
     DeviceBuffer scratch[kLanes];
-    // Split: a segment without carried state whose Disparity member is the
-    // full search runs each pair's census, costs and path volumes on lanes[0]
-    // and its selection onwards on lanes[1], so pair n + 1's path scan (bound
-    // by its steps' latency and the integer pipe) runs beside pair n's
-    // selection (bound by HBM). Requests alternate between the two scratches;
-    // carved[k]: scratch k's path volumes written, freed[k]: read.
+    // Split: a segment whose Disparity member is the full search, with no
+    // stage carrying state before it, runs each pair's census, costs and path
+    // volumes on lanes[0] and its selection onwards on lanes[1] (the stages
+    // carrying state among them, in request order), so pair n + 1's front half
+    // runs beside pair n's back half. Requests alternate between the two
+    // scratches; carved[k]: scratch k's path volumes written, freed[k]: read.
     bool split = false;
     cudaEvent_t carved[kLanes] = {}, freed[kLanes] = {};
     std::vector<void *> allocations;
@@ -1369,13 +1369,18 @@ extern "C" nxs_status nxs_configure(nxs_context *c, uint32_t id, const nxs_geome
     }
     cudaSetDevice(c->device);
     cudaError_t e = cudaSuccess;
-    bool carries = false;
-    for (const Member &m : seg->members)
-        carries = carries || m.kind == Kind::Temporal || m.kind == Kind::Quality;
-    seg->n_lanes = carries ? 1 : kLanes;
-    for (const Member &m : seg->members)
-        if (m.kind == Kind::Disparity && !m.coarse_to_fine && seg->n_lanes == 2 && g_split_lanes)
-            seg->split = true;
+    // Stages that carry state (TemporalFilter, Quality) keep it in request order
+    // on one stream: the whole pair's, or with the split the back stream's,
+    // where every stage after the Disparity member runs.
+    bool carries = false, carries_before = false, full_search = false;
+    for (const Member &m : seg->members) {
+        const bool stateful = m.kind == Kind::Temporal || m.kind == Kind::Quality;
+        carries = carries || stateful;
+        carries_before = carries_before || (stateful && !full_search);
+        full_search = full_search || (m.kind == Kind::Disparity && !m.coarse_to_fine);
+    }
+    seg->split = g_split_lanes && full_search && !carries_before;
+    seg->n_lanes = carries && !seg->split ? 1 : kLanes;
     for (cudaStream_t *st : {&seg->upload, &seg->download, &seg->notify})
         if (!e) e = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
     for (int k = 0; k < seg->n_lanes; ++k)

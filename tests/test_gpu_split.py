@@ -10,15 +10,26 @@ from tests import gpu_util as g
 pytestmark = pytest.mark.gpu
 
 
-def _run(split, pairs, frames_of, w, h):
-    from nx_stereo_b200 import native, segment, stage
+CHAIN = "cloud"  # the stateless chain; "state": the serving chain with temporal and quality
+
+
+def _stages(chain):
+    from nx_stereo_b200 import stage
+
+    if chain == "state":
+        return [stage.Rectification, (stage.Disparity, {"num_disparities": 128}),
+                stage.SpeckleFilter, stage.TemporalFilter, stage.Depth, stage.Quality]
+    return [stage.Rectification, (stage.Disparity, {"num_disparities": 128}),
+            stage.SpeckleFilter, stage.Depth, (stage.PointCloud, {"decimation": 4})]
+
+
+def _run(split, pairs, frames_of, w, h, chain=CHAIN):
+    from nx_stereo_b200 import native, segment
 
     native.load().nxs_set_split_lanes(1 if split else 0)
     try:
         geometry = segment.standard_geometry(w, h)
-        status, members = segment.members(
-            [stage.Rectification, (stage.Disparity, {"num_disparities": 128}),
-             stage.SpeckleFilter, stage.Depth, (stage.PointCloud, {"decimation": 4})], geometry)
+        status, members = segment.members(_stages(chain), geometry)
         assert status == "ok", members
         status, seg = segment.CudaSegment.build(members, geometry)
         assert status == "ok", seg
@@ -66,3 +77,27 @@ def test_split_equals_unsplit_and_the_oracle(oracle):
     d = np.where(d > 0, d, np.float32(-1.0)).astype(np.float32)
     want = oracle.despeckle(d, 12, 1.0, 3)
     assert g.same_bits(split[0]["disparity"], want)
+
+
+def test_split_keeps_the_state_in_order():
+    """The serving chain (TemporalFilter and Quality carry state from pair to
+    pair): split, its state advances on the back stream in request order, so
+    every pair's outputs equal those of the segment run on one stream."""
+    from nx_stereo_b200 import scene
+
+    w, h = 364, 272
+    rig = scene.rig(w, h)
+    frames = []
+    for k in range(5):
+        left, right = scene.rectified_pair(w, h, seed=130 + k, rectangles=6, max_disparity=56)
+        frames.append(scene.raw_frames(left, right, rig))
+
+    def frames_of(k):
+        return {"left_frame": frames[k % 5][0], "right_frame": frames[k % 5][1]}
+
+    split = _run(True, 8, frames_of, w, h, chain="state")
+    plain = _run(False, 8, frames_of, w, h, chain="state")
+    for a, b in zip(split, plain):
+        assert a.keys() == b.keys()
+        for key in a:
+            assert a[key].tobytes() == b[key].tobytes(), key
