@@ -263,7 +263,7 @@ constexpr int kSlots = 4;
 constexpr int kLanes = 2;
 // Whether segments configured from now on split their matcher over two
 // streams (Segment::split); set by nxs_set_split_lanes.
-static bool g_split_lanes = true;
+static std::atomic<bool> g_split_lanes{true};
 
 struct Segment {
     uint32_t id = 0;

@@ -12,6 +12,7 @@
 // writes D contiguous bytes: one coalesced 128-byte transaction per warp at
 // D = 128.
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <type_traits>
 
@@ -175,7 +176,7 @@ static bool encode_cost_maps(const uint8_t *costs, int width, int height, int di
 // where they measured faster (1280x720x128: 295 against 300 us, 1920x1080x256:
 // 1329 against 1360 us); below it the per-lane copies were (728x544x128: 121
 // against 129 us, 364x272x64: 40 against 53 us). Results do not depend on it.
-static int g_path_tiles = 1;
+static std::atomic<int> g_path_tiles{1};
 constexpr size_t kTilesFrom = (size_t)96 << 20;
 void set_path_tiles(int mode) { g_path_tiles = mode < 0 || mode > 2 ? 1 : mode; }
 int path_tiles() { return g_path_tiles; }
@@ -200,7 +201,7 @@ __global__ void __launch_bounds__(256) clear_kernel(uint4 *__restrict__ to, size
 
 // Words a path lane holds at each disparity count (4, 8 or 16), the tunable
 // shape of the path kernels; words_slot maps 64..256 to the table.
-static int g_path_words[5] = {8, 8, 8, 8, 8};
+static std::atomic<int> g_path_words[5] = {8, 8, 8, 8, 8};
 static int words_slot(int disparities) {
     return disparities <= 64 ? 0 : disparities <= 96 ? 1 : disparities <= 128 ? 2
                                    : disparities <= 192 ? 3 : 4;
@@ -329,7 +330,7 @@ cudaError_t launch_paths(const uint8_t *costs, int width, int height, int dispar
 // then selection over it. The reductions run at a few TB/s in L2, below what
 // the path volumes' plain stores reach, so 1 measured slower at every size
 // from 364x272x64 to 1920x1080x256 and is kept as a knob, not a default.
-static int g_path_sums = 0;
+static std::atomic<int> g_path_sums{0};
 void set_path_sums(int mode) { g_path_sums = mode == 1 ? 1 : 0; }
 int path_sums_mode() { return g_path_sums; }
 
