@@ -339,6 +339,8 @@ class Request:
         key = tuple(f[:7] + f[8:] for f in fields)
         layout = _LAYOUTS.get(key)
         if layout is None:
+            if len(_LAYOUTS) >= 256:
+                _LAYOUTS.clear()
             layout = [(ctypes.string_at(f[0]).decode(), np.dtype(DTYPES[f[1]]), tuple(f[3:3 + f[2]]),
                        f[8]) for f in fields]
             _LAYOUTS[key] = layout
@@ -445,6 +447,8 @@ class Context:
             cache = _local.entries = {}
         ts = cache.get(key)
         if ts is None:
+            if len(cache) >= 64:  # shapes come and go: keep the cache small
+                cache.clear()
             ts = (Tensor * max(len(arrays), 1))()
             names = [name.encode() for name in entries]
             for i, (b, a) in enumerate(zip(names, arrays)):
