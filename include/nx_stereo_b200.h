@@ -231,6 +231,13 @@ nxs_status nxs_set_path_tiles(uint32_t mode);
  * streams, pairs alternating, and one with state on one stream. Results do
  * not depend on it. */
 nxs_status nxs_set_split_lanes(uint32_t on);
+/* In split segments, the selection on the back stream runs with this many
+ * resident blocks a SM stepping through the pixel blocks (8 by default; 0:
+ * one block for each, all launched), so that it holds fewer warps beside the
+ * next pair's path scan; at most 16. A tuning knob; results do not depend on it.
+ * nxs_lean_select: the current setting. */
+nxs_status nxs_set_lean_select(uint32_t blocks_per_sm);
+uint32_t nxs_lean_select(void);
 uint32_t nxs_path_tiles(void);
 uint32_t nxs_path_wait_failures(void);
 

@@ -471,6 +471,14 @@ extern "C" uint32_t nxs_path_sums(uint32_t width, uint32_t height, uint32_t disp
     return path_sums_wanted((int)width, (int)height, (int)disparities) ? 1u : 0u;
 }
 
+extern "C" nxs_status nxs_set_lean_select(uint32_t blocks_per_sm) {
+    if (blocks_per_sm > 16) return NXS_BAD_ARGUMENT;
+    set_lean_select((int)blocks_per_sm);
+    return NXS_OK;
+}
+
+extern "C" uint32_t nxs_lean_select(void) { return (uint32_t)lean_select(); }
+
 extern "C" nxs_status nxs_set_split_lanes(uint32_t on) {
     if (on > 1) return NXS_BAD_ARGUMENT;
     g_split_lanes = on != 0;
@@ -1669,7 +1677,8 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
             if (!e) e = cudaStreamWaitEvent(back, seg->carved[lane], 0);
             if (!e)
                 e = run_matcher_back(g.width, g.height, m.disparities, m.paths,
-                                     l.sgm.uniqueness, 1, ms, slot.disparity[current], back);
+                                     l.sgm.uniqueness, 1, ms, slot.disparity[current], back,
+                                     true);
             if (!e) e = cudaEventRecord(seg->freed[lane], back);
             s = back;
             break;

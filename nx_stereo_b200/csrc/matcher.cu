@@ -401,14 +401,54 @@ __global__ void __launch_bounds__(128)
                                   disparity, keys, nullptr, blockIdx.x, values_of, one);
 }
 
+// select_kernel with a grid of `resident` blocks that step through the
+// pixel blocks: a selection run beside another stream's path scan holds
+// fewer warps a SM while it streams the path volumes.
+template <int G, int PATHS, int SPAN>
+__global__ void __launch_bounds__(128)
+    select_lean_kernel(const void *__restrict__ source, int width, int height, int disparities,
+                       size_t volume, float uniqueness, float *__restrict__ disparity,
+                       uint32_t *__restrict__ keys, uint32_t one, size_t blocks) {
+    follow_previous_grid();
+    __shared__ __align__(16) uint16_t values_of[128 / G][256];
+    for (size_t block = blockIdx.x; block < blocks; block += gridDim.x) {
+        __syncwarp();  // the group's row of values_of is read before it is rewritten
+        select_pixels<G, PATHS, SPAN>(source, width, height, disparities, volume, uniqueness,
+                                      disparity, keys, nullptr, block, values_of, one);
+    }
+}
+
+// Blocks a SM of the lean selection the split segments run beside a path scan
+// (0: one block for each pixel block). 8 measured best end to end on the
+// 728x544x128 chain: 2% above the full grid, 16 (above the 12 that fit a SM at
+// 39 registers) 7% below it.
+static std::atomic<int> g_lean_select{8};
+void set_lean_select(int blocks_per_sm) { g_lean_select = blocks_per_sm < 0 ? 0 : blocks_per_sm; }
+int lean_select() { return g_lean_select.load(); }
+
 template <int PATHS, int SPAN = 0>
 static cudaError_t launch_select(const void *source, int width, int height, int disparities,
                                  float uniqueness, float *disparity, uint32_t *keys,
-                                 cudaStream_t stream) {
+                                 cudaStream_t stream, int lean = 0) {
     const size_t pixels = (size_t)width * height;
     const size_t volume = pixels * disparities;
     const int g = group_lanes(disparities);
     const unsigned blocks = (unsigned)((pixels + 128 / g - 1) / (128 / g));
+    if (lean > 0) {
+        int device = 0, sms = 148;
+        cudaGetDevice(&device);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        const unsigned grid = std::min<unsigned>(blocks, (unsigned)(lean * sms));
+#define NXS_LEAN(G)                                                                            \
+    launch_after(select_lean_kernel<G, PATHS, SPAN>, dim3(grid), dim3(128), 0, stream, source,  \
+                 width, height, disparities, volume, uniqueness, disparity, keys, 1u,           \
+                 (size_t)blocks)
+        if (g == 4) NXS_LEAN(4);
+        else if (g == 8) NXS_LEAN(8);
+        else NXS_LEAN(16);
+#undef NXS_LEAN
+        return cudaGetLastError();
+    }
 #define NXS_SELECT(G)                                                                         \
     launch_after(select_kernel<G, PATHS, SPAN>, dim3(blocks), dim3(128), 0, stream, source,   \
                  width, height, disparities, volume, uniqueness, disparity, keys, 1u)
@@ -421,12 +461,12 @@ static cudaError_t launch_select(const void *source, int width, int height, int 
 
 cudaError_t launch_select_paths(const uint8_t *paths_in, int width, int height, int disparities,
                                 int paths, float uniqueness, float *disparity, uint32_t *keys,
-                                cudaStream_t stream, int span) {
+                                cudaStream_t stream, int span, int lean) {
 #define NXS_SELECT_SPAN(S)                                                                     \
     return paths == 8 ? launch_select<8, S>(paths_in, width, height, disparities, uniqueness,   \
-                                            disparity, keys, stream)                           \
+                                            disparity, keys, stream, lean)                     \
                       : launch_select<3, S>(paths_in, width, height, disparities, uniqueness,   \
-                                            disparity, keys, stream)
+                                            disparity, keys, stream, lean)
     if (span == 16) NXS_SELECT_SPAN(16);
     if (span == 8) NXS_SELECT_SPAN(8);
 #undef NXS_SELECT_SPAN
@@ -635,14 +675,15 @@ cudaError_t run_matcher_front(const uint8_t *left, const uint8_t *right, int wid
 
 cudaError_t run_matcher_back(int width, int height, int disparities, int paths,
                              float uniqueness, int stage_mask, const MatcherScratch &s,
-                             float *disparity, cudaStream_t stream) {
+                             float *disparity, cudaStream_t stream, bool beside) {
     cudaError_t e;
     if (path_sums_wanted(width, height, disparities))
         e = launch_select_path_sums(reinterpret_cast<const uint16_t *>(s.paths), width, height,
                                     disparities, uniqueness, s.selected, s.keys, stream);
     else
         e = launch_select_paths(s.paths, width, height, disparities, paths, uniqueness,
-                                s.selected, s.keys, stream, matcher_span(disparities));
+                                s.selected, s.keys, stream, matcher_span(disparities),
+                                beside ? g_lean_select.load() : 0);
     if (e) return e;
     return launch_check_median(s.selected, s.keys, width, height, stage_mask, disparity, stream);
 }

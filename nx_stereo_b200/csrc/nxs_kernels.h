@@ -68,9 +68,12 @@ unsigned path_wait_failures();
 // sums[y][x][d] = sum over paths of paths_in (u16).
 cudaError_t launch_sum_paths(const uint8_t *paths_in, int width, int height, int disparities,
                              int paths, uint16_t *sums, cudaStream_t stream);
+// lean > 0: that many resident blocks a SM step through the pixel blocks.
 cudaError_t launch_select_paths(const uint8_t *paths_in, int width, int height, int disparities,
                                 int paths, float uniqueness, float *disparity, uint32_t *keys,
-                                cudaStream_t stream, int span = 0);
+                                cudaStream_t stream, int span = 0, int lean = 0);
+void set_lean_select(int blocks_per_sm);
+int lean_select();
 cudaError_t launch_select_sums(const uint16_t *sums, int width, int height, int disparities,
                                float uniqueness, float *disparity, uint32_t *keys,
                                cudaStream_t stream);
@@ -140,7 +143,7 @@ cudaError_t run_matcher_front(const uint8_t *left, const uint8_t *right, int wid
                               const MatcherScratch &scratch, cudaStream_t stream);
 cudaError_t run_matcher_back(int width, int height, int disparities, int paths,
                              float uniqueness, int stage_mask, const MatcherScratch &scratch,
-                             float *disparity, cudaStream_t stream);
+                             float *disparity, cudaStream_t stream, bool beside = false);
 
 // ---- the coarse-to-fine search (band.cu) ----
 // Both images' rounded 2x2 means.

@@ -133,6 +133,8 @@ SIGNATURES = {
     "nxs_path_sums": (_u32, [_u32, _u32, _u32]),
     "nxs_set_path_tiles": (_i, [_u32]),
     "nxs_set_split_lanes": (_i, [_u32]),
+    "nxs_set_lean_select": (_i, [_u32]),
+    "nxs_lean_select": (_u32, []),
     "nxs_path_tiles": (_u32, []),
     "nxs_path_wait_failures": (_u32, []),
     "nxs_band_check": (_i, [ctypes.POINTER(BandParams), _u32, _u32, ctypes.c_int32] + _err),

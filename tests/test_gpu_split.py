@@ -23,10 +23,13 @@ def _stages(chain):
             stage.SpeckleFilter, stage.Depth, (stage.PointCloud, {"decimation": 4})]
 
 
-def _run(split, pairs, frames_of, w, h, chain=CHAIN):
+def _run(split, pairs, frames_of, w, h, chain=CHAIN, lean=None):
     from nx_stereo_b200 import native, segment
 
     native.load().nxs_set_split_lanes(1 if split else 0)
+    lean_before = native.load().nxs_lean_select()
+    if lean is not None:
+        assert native.load().nxs_set_lean_select(lean) == 0
     try:
         geometry = segment.standard_geometry(w, h)
         status, members = segment.members(_stages(chain), geometry)
@@ -47,6 +50,7 @@ def _run(split, pairs, frames_of, w, h, chain=CHAIN):
         return replies
     finally:
         native.load().nxs_set_split_lanes(1)
+        native.load().nxs_set_lean_select(lean_before)
 
 
 def test_split_equals_unsplit_and_the_oracle(oracle):
@@ -97,6 +101,31 @@ def test_split_keeps_the_state_in_order():
 
     split = _run(True, 8, frames_of, w, h, chain="state")
     plain = _run(False, 8, frames_of, w, h, chain="state")
+    for a, b in zip(split, plain):
+        assert a.keys() == b.keys()
+        for key in a:
+            assert a[key].tobytes() == b[key].tobytes(), key
+
+
+@pytest.mark.parametrize("lean", [0, 1, 3, 16])
+def test_lean_selection_is_the_same(lean):
+    """The selection a split segment runs beside the next pair's path scan, as a
+    grid of `lean` blocks a SM stepping through the pixel blocks (0: one block
+    for each), gives the same outputs as the segment on one stream."""
+    from nx_stereo_b200 import scene
+
+    w, h = 500, 301  # a ragged last pixel block
+    rig = scene.rig(w, h)
+    frames = []
+    for k in range(3):
+        left, right = scene.rectified_pair(w, h, seed=170 + k, rectangles=5, max_disparity=100)
+        frames.append(scene.raw_frames(left, right, rig))
+
+    def frames_of(k):
+        return {"left_frame": frames[k % 3][0], "right_frame": frames[k % 3][1]}
+
+    split = _run(True, 6, frames_of, w, h, lean=lean)
+    plain = _run(False, 6, frames_of, w, h)
     for a, b in zip(split, plain):
         assert a.keys() == b.keys()
         for key in a:
