@@ -25,6 +25,7 @@ each: p50/p99 latency).
 threads, one pair per thread per step.
 """
 import argparse
+import collections
 import gc
 import json
 import os
@@ -315,29 +316,36 @@ def run_ours(args, rank, world, local_rank):
     h2d = sum(a.nbytes for a in entries[0].values())
     d2h = None
 
-    def e2e_loop(count):
+    inflight = collections.deque()
+    sent = 0
+
+    def take_reply():
         nonlocal d2h
-        inflight = []
-        for i in range(count):
-            status, req = mod.send_request(entries[i % len(entries)], seg)
+        reply = mod.await_(inflight.popleft(), seg, 60000)
+        assert reply[0] == "ok", reply
+        d2h = sum(v.nbytes for v in reply[1].values())
+
+    def e2e_send(count):
+        """Sends `count` pairs, awaiting the oldest whenever depth are in flight."""
+        nonlocal sent
+        for _ in range(count):
+            status, req = mod.send_request(entries[sent % len(entries)], seg)
             assert status == "ok", req
+            sent += 1
             inflight.append(req)
             if len(inflight) >= mod.depth():
-                reply = mod.await_(inflight.pop(0), seg, 60000)
-                assert reply[0] == "ok", reply
-                d2h = sum(v.nbytes for v in reply[1].values())
-        while inflight:
-            reply = mod.await_(inflight.pop(0), seg, 60000)
-            assert reply[0] == "ok", reply
-            d2h = sum(v.nbytes for v in reply[1].values())
+                take_reply()
 
-    e2e_loop(max(args.warmup, mod.depth()))
+    e2e_send(max(args.warmup, mod.depth()))
+    while inflight:
+        take_reply()
     torch.cuda.synchronize()
     replicas.barrier()
     # The cyclic collector paused for the timed loop, as the serving loop does:
     # a collection of the replies' objects stalls the host for milliseconds.
-    # The loop sends --steps pairs at a time until it has run E2E_MIN_SECONDS;
-    # every rank runs the same number of rounds (the first rank's count).
+    # The loop sends --steps pairs at a time, keeping depth pairs in flight from
+    # one round to the next, until it has run E2E_MIN_SECONDS; then it takes the
+    # last replies. Every rank runs the same number of rounds (the first rank's).
     collecting = gc.isenabled()
     gc.disable()
     try:
@@ -345,12 +353,13 @@ def run_ours(args, rank, world, local_rank):
         c0 = time.thread_time()  # the calling thread's CPU time: the API's host cost
         e2e_pairs = 0
         while True:
-            e2e_loop(args.steps)
+            e2e_send(args.steps)
             e2e_pairs += args.steps
-            torch.cuda.synchronize()
             more = time.perf_counter() - e0 < E2E_MIN_SECONDS
             if not replicas.agree(more, device="cuda"):
                 break
+        while inflight:
+            take_reply()
         e_elapsed = time.perf_counter() - e0
         host_cpu_s = time.thread_time() - c0
         e1 = time.monotonic()
