@@ -13,17 +13,17 @@ pytestmark = pytest.mark.gpu
 CHAIN = "cloud"  # the stateless chain; "state": the serving chain with temporal and quality
 
 
-def _stages(chain):
+def _stages(chain, disparities=128):
     from nx_stereo_b200 import stage
 
     if chain == "state":
         return [stage.Rectification, (stage.Disparity, {"num_disparities": 128}),
                 stage.SpeckleFilter, stage.TemporalFilter, stage.Depth, stage.Quality]
-    return [stage.Rectification, (stage.Disparity, {"num_disparities": 128}),
+    return [stage.Rectification, (stage.Disparity, {"num_disparities": disparities}),
             stage.SpeckleFilter, stage.Depth, (stage.PointCloud, {"decimation": 4})]
 
 
-def _run(split, pairs, frames_of, w, h, chain=CHAIN, lean=None):
+def _run(split, pairs, frames_of, w, h, chain=CHAIN, lean=None, disparities=128):
     from nx_stereo_b200 import native, segment
 
     native.load().nxs_set_split_lanes(1 if split else 0)
@@ -32,7 +32,7 @@ def _run(split, pairs, frames_of, w, h, chain=CHAIN, lean=None):
         assert native.load().nxs_set_lean_select(lean) == 0
     try:
         geometry = segment.standard_geometry(w, h)
-        status, members = segment.members(_stages(chain), geometry)
+        status, members = segment.members(_stages(chain, disparities), geometry)
         assert status == "ok", members
         status, seg = segment.CudaSegment.build(members, geometry)
         assert status == "ok", seg
@@ -130,3 +130,30 @@ def test_lean_selection_is_the_same(lean):
         assert a.keys() == b.keys()
         for key in a:
             assert a[key].tobytes() == b[key].tobytes(), key
+
+
+@pytest.mark.parametrize("disparities", [64, 256])
+def test_lean_selection_other_lane_counts(disparities):
+    """The lean selection with 4 and 16 lanes a pixel (64 and 256 disparities),
+    at its default setting and with one block a SM, against the segment on one
+    stream."""
+    from nx_stereo_b200 import scene
+
+    w, h = 420, 197
+    rig = scene.rig(w, h)
+    frames = []
+    for k in range(3):
+        left, right = scene.rectified_pair(w, h, seed=190 + k, rectangles=5,
+                                           max_disparity=min(disparities - 8, 200))
+        frames.append(scene.raw_frames(left, right, rig))
+
+    def frames_of(k):
+        return {"left_frame": frames[k % 3][0], "right_frame": frames[k % 3][1]}
+
+    plain = _run(False, 5, frames_of, w, h, disparities=disparities)
+    for lean in (None, 1):
+        split = _run(True, 5, frames_of, w, h, lean=lean, disparities=disparities)
+        for a, b in zip(split, plain):
+            assert a.keys() == b.keys()
+            for key in a:
+                assert a[key].tobytes() == b[key].tobytes(), (lean, key)
