@@ -166,7 +166,9 @@ class ClockSampler:
 # ---------------------------------------------------------------- our arm
 class DevicePipeline:
     """The pipeline's kernels on device buffers, one C-ABI call per stage; CUDA
-    events bracket the path-aggregation kernel (the dominant one)."""
+    events bracket the path-aggregation kernel (the dominant one). The
+    rectification maps are the stream's state, made once for its cameras and
+    kept on the device, as a segment keeps them."""
 
     def __init__(self, native, torch, ctx, rig, stream, aggregate="volumes"):
         from nx_stereo_b200 import scene
@@ -196,6 +198,12 @@ class DevicePipeline:
         self.kept = torch.empty(1, dtype=torch.int32, device=dev)
         # The costs and path volumes in the order the matcher itself keeps them.
         self.span = int(native.load().nxs_matcher_span(DISPARITIES))
+        import ctypes
+
+        self.maps = torch.empty((2, HEIGHT, WIDTH, 2), dtype=f32, device=dev)
+        native.call("nxs_rectify_maps_device", ctypes.byref(self.cameras[0]),
+                    ctypes.byref(self.cameras[1]), WIDTH, HEIGHT, WIDTH, HEIGHT,
+                    self.maps.data_ptr(), stream)
 
     STAGES = ["rectify", "census_costs", "paths", "select", "check_median",
               "despeckle_depth_cloud"]
@@ -214,9 +222,9 @@ class DevicePipeline:
                 marks[i].record()
 
         mark(0)
-        call("nxs_rectify_pair_device", frames[0].data_ptr(), frames[1].data_ptr(), WIDTH,
-             HEIGHT, ctypes.byref(self.cameras[0]), ctypes.byref(self.cameras[1]), WIDTH, HEIGHT,
-             self.images[0].data_ptr(), self.images[1].data_ptr(), s)
+        call("nxs_rectify_pair_mapped_device", frames[0].data_ptr(), frames[1].data_ptr(), WIDTH,
+             HEIGHT, self.maps.data_ptr(), WIDTH, HEIGHT, self.images[0].data_ptr(),
+             self.images[1].data_ptr(), s)
         mark(1)
         call("nxs_census_costs_device_ordered", self.images[0].data_ptr(),
              self.images[1].data_ptr(), WIDTH, HEIGHT, DISPARITIES, self.span,

@@ -455,6 +455,21 @@ nxs_status nxs_rectify_pair_device(const uint8_t *d_left_frame, const uint8_t *d
                                    uint32_t height, uint8_t *d_left, uint8_t *d_right,
                                    void *stream);
 
+/* The rectification split in two: the frame position every rectified pixel of
+ * both sides samples, d_maps[side][y][x] = (x, y) as f32 (2 x height x width
+ * pairs, 8-byte aligned; a function of the cameras and sizes alone), then the
+ * pair sampled from its frames through them. The two give nxs_rectify_pair_device's
+ * bytes; a segment keeps the maps on the device and remakes them only when a
+ * request's cameras change. */
+nxs_status nxs_rectify_maps_device(const nxs_camera *left, const nxs_camera *right,
+                                   uint32_t frame_width, uint32_t frame_height, uint32_t width,
+                                   uint32_t height, float *d_maps, void *stream);
+nxs_status nxs_rectify_pair_mapped_device(const uint8_t *d_left_frame,
+                                          const uint8_t *d_right_frame, uint32_t frame_width,
+                                          uint32_t frame_height, const float *d_maps,
+                                          uint32_t width, uint32_t height, uint8_t *d_left,
+                                          uint8_t *d_right, void *stream);
+
 /* NxStereo.Filter.despeckle/2 (lib/nx_stereo/filter.ex:14-80); radius 1..8. */
 nxs_status nxs_despeckle_device(const float *d_disparity, uint32_t width, uint32_t height,
                                 float min_support, float max_diff, uint32_t radius,

@@ -303,6 +303,12 @@ struct Segment {
     // scratches; carved[k]: scratch k's path volumes written, freed[k]: read.
     bool split = false;
     cudaEvent_t carved[kLanes] = {}, freed[kLanes] = {};
+    // The Rectification member's maps (the frame position each rectified pixel
+    // samples, both sides), one per compute lane and rewritten on that lane's
+    // stream when a request's cameras differ from those it was made for.
+    float2 *rectify_maps[kLanes] = {};
+    Camera rectify_cameras[kLanes][2];
+    bool rectify_mapped[kLanes] = {};
     std::vector<void *> allocations;
 
     std::vector<cudaStream_t> streams() const {
@@ -893,6 +899,8 @@ extern "C" nxs_status nxs_median3_device(const float *d_image, uint32_t width, u
                : NXS_OK;
 }
 
+static_assert(sizeof(Camera) == 23 * sizeof(float), "cameras compare as their bytes");
+
 static Camera to_camera(const nxs_camera *c) {
     Camera k;
     memcpy(k.k, c->k, sizeof k.k);
@@ -924,6 +932,35 @@ extern "C" nxs_status nxs_rectify_pair_device(const uint8_t *d_left_frame,
     return launch_rectify_pair(d_left_frame, d_right_frame, frame_width, frame_height,
                                to_camera(left), to_camera(right), width, height, d_left, d_right,
                                static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_rectify_maps_device(const nxs_camera *left, const nxs_camera *right,
+                                              uint32_t frame_width, uint32_t frame_height,
+                                              uint32_t width, uint32_t height, float *d_maps,
+                                              void *stream) {
+    CHECK_SIZE(left && right && d_maps && (uintptr_t)d_maps % 8 == 0 && width > 0 &&
+               height > 0 && frame_width >= width && frame_height >= height);
+    return launch_rectify_maps(to_camera(left), to_camera(right), frame_width, frame_height,
+                               width, height, reinterpret_cast<float2 *>(d_maps),
+                               static_cast<cudaStream_t>(stream))
+               ? NXS_CUDA_ERROR
+               : NXS_OK;
+}
+
+extern "C" nxs_status nxs_rectify_pair_mapped_device(const uint8_t *d_left_frame,
+                                                     const uint8_t *d_right_frame,
+                                                     uint32_t frame_width, uint32_t frame_height,
+                                                     const float *d_maps, uint32_t width,
+                                                     uint32_t height, uint8_t *d_left,
+                                                     uint8_t *d_right, void *stream) {
+    CHECK_SIZE(d_left_frame && d_right_frame && d_maps && (uintptr_t)d_maps % 8 == 0 &&
+               d_left && d_right && width > 0 && height > 0 && frame_width >= width &&
+               frame_height >= height);
+    return launch_rectify_mapped(d_left_frame, d_right_frame, frame_width, frame_height,
+                                 reinterpret_cast<const float2 *>(d_maps), width, height, d_left,
+                                 d_right, static_cast<cudaStream_t>(stream))
                ? NXS_CUDA_ERROR
                : NXS_OK;
 }
@@ -1479,7 +1516,10 @@ extern "C" nxs_status nxs_configure(nxs_context *c, uint32_t id, const nxs_geome
         for (cudaEvent_t *ev : {&slot.entered, &slot.free})
             if (!e) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
     }
+    const bool rectifies = std::any_of(seg->members.begin(), seg->members.end(),
+                                       [](const Member &m) { return m.kind == Kind::Rectification; });
     for (int k = 0; k < seg->n_lanes; ++k) {
+        if (!e && rectifies) e = seg->alloc(&seg->rectify_maps[k], 2 * pixels);
         if (!e) e = seg->alloc(&seg->depth_m[k], pixels);
         if (!e && max_disparities) e = seg->scratch[k].reserve(matcher_scratch);
         for (cudaEvent_t *ev : {&seg->carved[k], &seg->freed[k]})
@@ -1645,11 +1685,26 @@ extern "C" nxs_status nxs_run_async(nxs_context *c, uint32_t id, uint32_t n_memb
         e = cudaEventRecord(r->marks[i], s);
         if (e) break;
         switch (m.kind) {
-        case Kind::Rectification:
-            e = launch_rectify_pair(slot.frames[0], slot.frames[1], g.frame_width, g.frame_height,
-                                    l.cameras[0], l.cameras[1], g.width, g.height,
-                                    slot.images[0], slot.images[1], s);
+        case Kind::Rectification: {
+            // The map of the lane whose stream runs this, remade only for new cameras.
+            const int k = seg->n_lanes > 1 && s == seg->lanes[1] ? 1 : 0;
+            if (!seg->rectify_mapped[k] ||
+                memcmp(seg->rectify_cameras[k], l.cameras, sizeof l.cameras) != 0) {
+                seg->rectify_mapped[k] = false;
+                e = launch_rectify_maps(l.cameras[0], l.cameras[1], g.frame_width,
+                                        g.frame_height, g.width, g.height, seg->rectify_maps[k],
+                                        s);
+                if (!e) {
+                    memcpy(seg->rectify_cameras[k], l.cameras, sizeof l.cameras);
+                    seg->rectify_mapped[k] = true;
+                }
+            }
+            if (!e)
+                e = launch_rectify_mapped(slot.frames[0], slot.frames[1], g.frame_width,
+                                          g.frame_height, seg->rectify_maps[k], g.width, g.height,
+                                          slot.images[0], slot.images[1], s);
             break;
+        }
         case Kind::Disparity: {
             if (m.coarse_to_fine) {
                 e = run_coarse_to_fine(slot.images[0], slot.images[1], g.width, g.height, m.paths,

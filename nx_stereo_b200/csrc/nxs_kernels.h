@@ -86,6 +86,16 @@ cudaError_t launch_median3(const float *image, int width, int height, int stage_
                            float *filtered, cudaStream_t stream);
 
 // ---- the stages around it ----
+// The frame positions both sides' rectified pixels sample, maps[side][v][u]
+// (2 x height x width), and the pair rectified from them: launch_rectify_maps
+// then launch_rectify_mapped gives launch_rectify_pair's bytes.
+cudaError_t launch_rectify_maps(const Camera &left_camera, const Camera &right_camera,
+                                int frame_width, int frame_height, int width, int height,
+                                float2 *maps, cudaStream_t stream);
+cudaError_t launch_rectify_mapped(const uint8_t *left_frame, const uint8_t *right_frame,
+                                  int frame_width, int frame_height, const float2 *maps,
+                                  int width, int height, uint8_t *left, uint8_t *right,
+                                  cudaStream_t stream);
 // Both sides of a pair in one launch (scale as launch_rectify).
 cudaError_t launch_rectify_pair(const uint8_t *left_frame, const uint8_t *right_frame,
                                 int frame_width, int frame_height, const Camera &left_camera,

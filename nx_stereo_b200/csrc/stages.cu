@@ -14,12 +14,11 @@ namespace nxs {
 // summed as 1 + (k3 r2^3 + (k2 r2^2 + k1 r2)), the order of Nx's expression,
 // native/stereo_match/src/rectify.rs:116-121) and the camera matrix; it is
 // scaled to the frame size at pixel centres and sampled bilinearly with 0
-// outside, then rounded half away from zero and clipped to u8.
-__device__ __forceinline__ void rectify_at(const uint8_t *__restrict__ frame, int frame_width,
-                                           int frame_height, const Camera &camera, float scale_x,
-                                           float scale_y, int width,
-                                           uint8_t *__restrict__ rectified, int u, int v) {
-    if (u >= width) return;
+// outside, then rounded half away from zero and clipped to u8. rectify_source
+// is the frame position a pixel samples (a function of the camera alone, so a
+// segment keeps it as a map), rectify_sample the sample there.
+__device__ __forceinline__ float2 rectify_source(const Camera &camera, float scale_x,
+                                                 float scale_y, int u, int v) {
     const float uf = (float)u, vf = (float)v;
     const float *ir = camera.inverse_pr;
     float x = fadd(fadd(fmul(ir[0], uf), fmul(ir[1], vf)), ir[2]);
@@ -40,8 +39,13 @@ __device__ __forceinline__ void rectify_at(const uint8_t *__restrict__ frame, in
     const float *k = camera.k;
     const float map_x = fadd(fadd(fmul(k[0], xd), fmul(k[1], yd)), k[2]);
     const float map_y = fadd(fmul(k[4], yd), k[5]);
-    const float source_x = fsub(fmul(fadd(map_x, 0.5f), scale_x), 0.5f);
-    const float source_y = fsub(fmul(fadd(map_y, 0.5f), scale_y), 0.5f);
+    return make_float2(fsub(fmul(fadd(map_x, 0.5f), scale_x), 0.5f),
+                       fsub(fmul(fadd(map_y, 0.5f), scale_y), 0.5f));
+}
+
+__device__ __forceinline__ uint8_t rectify_sample(const uint8_t *__restrict__ frame,
+                                                  int frame_width, int frame_height,
+                                                  float source_x, float source_y) {
     const float fx0 = floorf(source_x), fy0 = floorf(source_y);
     const float wx = fsub(source_x, fx0), wy = fsub(source_y, fy0);
     // float -> int as the reference casts: saturating, NaN to 0.
@@ -58,7 +62,17 @@ __device__ __forceinline__ void rectify_at(const uint8_t *__restrict__ frame, in
     const float value = fadd(fmul(fsub(1.0f, wy), top), fmul(wy, bottom));
     float r = roundf(value);
     r = r < 0.0f ? 0.0f : (r > 255.0f ? 255.0f : r);
-    rectified[(size_t)v * width + u] = (uint8_t)r;
+    return (uint8_t)r;
+}
+
+__device__ __forceinline__ void rectify_at(const uint8_t *__restrict__ frame, int frame_width,
+                                           int frame_height, const Camera &camera, float scale_x,
+                                           float scale_y, int width,
+                                           uint8_t *__restrict__ rectified, int u, int v) {
+    if (u >= width) return;
+    const float2 source = rectify_source(camera, scale_x, scale_y, u, v);
+    rectified[(size_t)v * width + u] =
+        rectify_sample(frame, frame_width, frame_height, source.x, source.y);
 }
 
 __global__ void rectify_kernel(const uint8_t *__restrict__ frame, int frame_width,
@@ -101,6 +115,58 @@ cudaError_t launch_rectify_pair(const uint8_t *left_frame, const uint8_t *right_
     dim3 grid((width + 127) / 128, height, 2);
     return launch_after(rectify_pair_kernel, grid, dim3(128), 0, stream, sides, frame_width,
                         frame_height, scale_x, scale_y, width);
+}
+
+// The maps of both sides: maps[side][v][u] = the frame position rectified
+// pixel (u, v) samples, side 0 through `left`, 1 through `right`.
+struct RectifyCameras {
+    Camera camera[2];
+};
+
+__global__ void rectify_maps_kernel(const RectifyCameras cameras, float scale_x, float scale_y,
+                                    int width, int height, float2 *__restrict__ maps) {
+    follow_previous_grid();
+    const int side = blockIdx.z, u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (u >= width) return;
+    maps[((size_t)side * height + v) * width + u] =
+        rectify_source(cameras.camera[side], scale_x, scale_y, u, v);
+}
+
+__global__ void rectify_mapped_kernel(const RectifySides sides, const float2 *__restrict__ maps,
+                                      int frame_width, int frame_height, int width, int height) {
+    follow_previous_grid();
+    const int side = blockIdx.z, u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (u >= width) return;
+    const float2 source = __ldg(maps + ((size_t)side * height + v) * width + u);
+    sides.rectified[side][(size_t)v * width + u] =
+        rectify_sample(sides.frame[side], frame_width, frame_height, source.x, source.y);
+}
+
+cudaError_t launch_rectify_maps(const Camera &left_camera, const Camera &right_camera,
+                                int frame_width, int frame_height, int width, int height,
+                                float2 *maps, cudaStream_t stream) {
+    RectifyCameras cameras;
+    cameras.camera[0] = left_camera;
+    cameras.camera[1] = right_camera;
+    const float scale_x = (float)((double)frame_width / (double)width);
+    const float scale_y = (float)((double)frame_height / (double)height);
+    dim3 grid((width + 127) / 128, height, 2);
+    return launch_after(rectify_maps_kernel, grid, dim3(128), 0, stream, cameras, scale_x,
+                        scale_y, width, height, maps);
+}
+
+cudaError_t launch_rectify_mapped(const uint8_t *left_frame, const uint8_t *right_frame,
+                                  int frame_width, int frame_height, const float2 *maps,
+                                  int width, int height, uint8_t *left, uint8_t *right,
+                                  cudaStream_t stream) {
+    RectifySides sides{};
+    sides.frame[0] = left_frame;
+    sides.frame[1] = right_frame;
+    sides.rectified[0] = left;
+    sides.rectified[1] = right;
+    dim3 grid((width + 127) / 128, height, 2);
+    return launch_after(rectify_mapped_kernel, grid, dim3(128), 0, stream, sides, maps,
+                        frame_width, frame_height, width, height);
 }
 
 cudaError_t launch_rectify(const uint8_t *frame, int frame_width, int frame_height,

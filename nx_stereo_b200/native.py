@@ -165,6 +165,9 @@ SIGNATURES = {
     "nxs_rectify_device": (_i, [_P, _u32, _u32, ctypes.POINTER(Camera), _u32, _u32, _P, _P]),
     "nxs_rectify_pair_device": (_i, [_P, _P, _u32, _u32, ctypes.POINTER(Camera),
                                      ctypes.POINTER(Camera), _u32, _u32, _P, _P, _P]),
+    "nxs_rectify_maps_device": (_i, [ctypes.POINTER(Camera), ctypes.POINTER(Camera), _u32, _u32,
+                                     _u32, _u32, _P, _P]),
+    "nxs_rectify_pair_mapped_device": (_i, [_P, _P, _u32, _u32, _P, _u32, _u32, _P, _P, _P]),
     "nxs_despeckle_device": (_i, [_P, _u32, _u32, _f, _f, _u32, _P, _P]),
     "nxs_temporal_device": (_i, [_P, _P, _P, _u64, _f, _f, _f, _f, _P]),
     "nxs_depth_device": (_i, [_P, _u64, _f, _f, _P, _P, _P]),

@@ -316,3 +316,19 @@ def test_coarse_to_fine_settings_and_refusals():
     for given, g, why in refusals:
         status, message = stage.Disparity.init(given, g)
         assert status == "error" and why in message, (given, message)
+
+
+def test_rectify_map_entries_refuse_bad_arguments():
+    # The maps are 8-byte (x, y) f32 pairs; sizes as the pair rectification's.
+    cam = native.make_camera([873.0, 0.0, 4.0, 0.0, 873.0, 4.0, 0.0, 0.0, 1.0],
+                             [0.0] * 5, [1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0])
+    lib = native.load()
+    ref = ctypes.byref(cam)
+    for maps, size, frame in [(0, (8, 8), (8, 8)), (4, (8, 8), (8, 8)),
+                              (4096, (0, 8), (8, 8)), (4096, (8, 8), (7, 8))]:
+        (w, h), (fw, fh) = size, frame
+        assert lib.nxs_rectify_maps_device(ref, ref, fw, fh, w, h, maps, None) == \
+            native.BAD_ARGUMENT, (maps, size, frame)
+        assert lib.nxs_rectify_pair_mapped_device(4096, 4096, fw, fh, maps, w, h, 4096, 4096,
+                                                  None) == native.BAD_ARGUMENT
+    assert lib.nxs_rectify_maps_device(None, ref, 8, 8, 8, 8, 4096, None) == native.BAD_ARGUMENT
