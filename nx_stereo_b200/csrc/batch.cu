@@ -599,7 +599,7 @@ cudaError_t fork_chains(nxs_batch *b, int *failed_pair) {
         const cudaError_t e = run_matcher(
             P.left, P.right, (int)s.width, (int)s.height, (int)s.params.disparities,
             (int)s.params.paths, (int)s.params.p1, (int)s.params.p2, s.params.uniqueness,
-            s.params.stage_mask ? 1 : 0, scratch, P.disparity, b->side[k]);
+            s.params.stage_mask ? 1 : 0, scratch, P.disparity, b->side[k], streams > 1);
         if (e != cudaSuccess && first == cudaSuccess) {
             first = e;
             *failed_pair = i;

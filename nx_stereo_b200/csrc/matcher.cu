@@ -691,12 +691,12 @@ cudaError_t run_matcher_back(int width, int height, int disparities, int paths,
 cudaError_t run_matcher(const uint8_t *left, const uint8_t *right, int width, int height,
                         int disparities, int paths, int p1, int p2, float uniqueness,
                         int stage_mask, const MatcherScratch &s, float *disparity,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, bool beside) {
     const cudaError_t e =
         run_matcher_front(left, right, width, height, disparities, paths, p1, p2, s, stream);
     if (e) return e;
     return run_matcher_back(width, height, disparities, paths, uniqueness, stage_mask, s,
-                            disparity, stream);
+                            disparity, stream, beside);
 }
 
 }  // namespace nxs

@@ -140,11 +140,13 @@ size_t matcher_scratch_bytes(int width, int height, int disparities);
 MatcherScratch carve_matcher_scratch(void *base, int width, int height, int disparities);
 
 // The whole matcher on device buffers: census, costs, paths, selection, the
-// check and the median (with Stage.Disparity's mask when stage_mask).
+// check and the median (with Stage.Disparity's mask when stage_mask). beside:
+// the selection runs beside other pairs' path scans (the lean grid of
+// set_lean_select).
 cudaError_t run_matcher(const uint8_t *left, const uint8_t *right, int width, int height,
                         int disparities, int paths, int p1, int p2, float uniqueness,
                         int stage_mask, const MatcherScratch &scratch, float *disparity,
-                        cudaStream_t stream);
+                        cudaStream_t stream, bool beside = false);
 // Its two halves: the census, costs and path volumes (front); selection, the
 // check and the median from the path volumes (back). run_matcher runs both on
 // one stream; a segment may run them on two, pairs apart.
