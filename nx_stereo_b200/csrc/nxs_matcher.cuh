@@ -212,6 +212,11 @@ __host__ __device__ inline size_t costs_shared_bytes(int disparities) {
 // group (run q of pixel p at (q + p / 4) mod D / 16), so a warp's 16-byte stores
 // to four pixel rows fall in 8 different bank quads; the write-out undoes the
 // rotation.
+// 256^b for the byte b of a word of costs, read at run time so that the
+// packing below stays multiply-adds (FMA pipe) beside the popcounts (XU) and
+// the XORs (integer pipe).
+__constant__ uint32_t g_byte_scale[4] = {1u, 256u, 65536u, 16777216u};
+
 template <int SPAN, int PIXELS>
 __device__ __forceinline__ void costs_from_codes(const uint64_t *lefts, const uint64_t *rights,
                                                  int width, int disparities,
@@ -245,16 +250,28 @@ __device__ __forceinline__ void costs_from_codes(const uint64_t *lefts, const ui
                                 (uint64_t)l23.z | (uint64_t)l23.w << 32};
         int rotated = q + group - chunks * (int)divide_small(group, magic);  // q + group % chunks
         if (rotated >= chunks) rotated -= chunks;
+        uint32_t scale[4];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) scale[b] = g_byte_scale[b];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             uint32_t words[4];
 #pragma unroll
             for (int w4 = 0; w4 < 4; ++w4) {
+                // Byte b of the word: the popcounts of the XOR's two halves, each
+                // added as count x 256^b (a cost is at most 48, so no byte carries).
                 uint32_t w = 0;
 #pragma unroll
                 for (int b = 0; b < 4; ++b) {
                     const int k = span_disparity(SPAN, 4 * w4 + b);
-                    w |= (uint32_t)__popcll(l4[i] ^ window[16 + i - k]) << (8 * b);
+                    const uint64_t x = l4[i] ^ window[16 + i - k];
+                    uint32_t low;
+                    asm("mad.lo.u32 %0, %1, %2, %3;"
+                        : "=r"(low)
+                        : "r"((uint32_t)__popc((uint32_t)x)), "r"(scale[b]), "r"(w));
+                    asm("mad.lo.u32 %0, %1, %2, %3;"
+                        : "=r"(w)
+                        : "r"((uint32_t)__popc((uint32_t)(x >> 32))), "r"(scale[b]), "r"(low));
                 }
                 words[w4] = w;
             }
