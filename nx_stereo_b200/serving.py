@@ -46,22 +46,34 @@ def percentile(values, p):
 
 
 def stream_bytes(geometry, stages, depth):
-    """Device bytes a stream's segment holds: its matcher's volumes (census
-    codes, costs, 8 path volumes, per-pixel maps) and `depth` slots of frames,
-    images and per-pixel outputs, plus the carried state."""
+    """Device bytes a stream's segment holds: for each compute lane its
+    matcher's volumes (costs, path volumes, per-pixel maps), its depth map and,
+    with a Rectification member, its rectification maps; `depth` slots of
+    frames, images and per-pixel outputs; the carried state. A segment has two
+    compute lanes unless a stage carrying state keeps it on one (no split
+    matcher: a carrying stage before the Disparity member, or no full search)."""
     from . import native
 
     w, h = geometry["width"], geometry["height"]
     fw, fh = geometry.get("frame_width", w), geometry.get("frame_height", h)
     d = 64
-    for entry in stages:
-        if isinstance(entry, tuple) and entry[0] is stage_module.Disparity:
-            d = int(entry[1].get("num_disparities", 64))
+    modules = [entry[0] if isinstance(entry, tuple) else entry for entry in stages]
+    full_search, carries, carries_before = False, False, False
+    for entry, module in zip(stages, modules):
+        settings = entry[1] if isinstance(entry, tuple) else {}
+        if module is stage_module.Disparity:
+            d = int(settings.get("num_disparities", 64))
+            full_search = settings.get("search", "full") != "coarse_to_fine"
+            carries_before = carries
+        if module in (stage_module.TemporalFilter, stage_module.Quality):
+            carries = True
+    lanes = 1 if carries and (carries_before or not full_search) else 2
     px = w * h
     scratch = int(native.load().nxs_sgm_scratch_bytes(w, h, d))
+    maps = 16 * px if stage_module.Rectification in modules else 0
     slot = 2 * fw * fh + 2 * px + 4 * (4 * px) + 2 * px
     carried = 4 * (4 * px)
-    return scratch + depth * slot + carried + 4 * px
+    return lanes * (scratch + 4 * px + maps) + depth * slot + carried
 
 
 Completed = collections.namedtuple("Completed", "stream seq arrival_ns done_ns outputs")
