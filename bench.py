@@ -26,6 +26,7 @@ threads, one pair per thread per step.
 """
 import argparse
 import collections
+import ctypes
 import gc
 import json
 import os
@@ -198,8 +199,6 @@ class DevicePipeline:
         self.kept = torch.empty(1, dtype=torch.int32, device=dev)
         # The costs and path volumes in the order the matcher itself keeps them.
         self.span = int(native.load().nxs_matcher_span(DISPARITIES))
-        import ctypes
-
         self.maps = torch.empty((2, HEIGHT, WIDTH, 2), dtype=f32, device=dev)
         native.call("nxs_rectify_maps_device", ctypes.byref(self.cameras[0]),
                     ctypes.byref(self.cameras[1]), WIDTH, HEIGHT, WIDTH, HEIGHT,
@@ -213,8 +212,6 @@ class DevicePipeline:
         stages. An event between two kernels also ends the overlap of the
         second's launch with the first's tail (programmatic dependent launch),
         so the timed steps record only the step's ends and the path stage."""
-        import ctypes
-
         s, call = self.stream, self.native.call
 
         def mark(i):
