@@ -133,3 +133,27 @@ def test_a_cap_on_pairs_in_flight_sends_the_oldest_arrivals_first():
         assert server.in_flight() <= 3
     assert [r["entries"]["frame"] for r in device.sent] == [0, 1, 2, 3, 4, 5]
     assert server.max_in_flight == 3
+
+
+def test_stream_bytes_count_each_compute_lane():
+    """A segment holds a matcher scratch, a depth map and, with a Rectification
+    member, rectification maps for each compute lane: two lanes unless a stage
+    carrying state keeps it on one (a carrying stage before the Disparity member,
+    or the coarse-to-fine search with one after it)."""
+    from nx_stereo_b200 import native, stage
+
+    g = {"width": 728, "height": 544}
+    px = 728 * 544
+    lane = int(native.load().nxs_sgm_scratch_bytes(728, 544, 128)) + 4 * px
+    full = (stage.Disparity, {"num_disparities": 128})
+    c2f = (stage.Disparity, {"num_disparities": 128, "search": "coarse_to_fine"})
+    base = serving.stream_bytes(g, [full], 4)
+    # stateless: two lanes; the state after a full search: still two (the split matcher)
+    assert serving.stream_bytes(g, [full, stage.Depth], 4) == base
+    assert serving.stream_bytes(g, [full, stage.TemporalFilter], 4) == base
+    # the state before the matcher, or after a coarse-to-fine search: one lane
+    assert serving.stream_bytes(g, [stage.TemporalFilter, full], 4) == base - lane
+    assert serving.stream_bytes(g, [c2f, stage.Quality], 4) == base - lane
+    assert serving.stream_bytes(g, [c2f], 4) == base
+    # the rectification maps: 2 sides x (x, y) f32 a pixel, each lane
+    assert serving.stream_bytes(g, [stage.Rectification, full], 4) == base + 2 * 16 * px
