@@ -332,3 +332,26 @@ def test_rectify_map_entries_refuse_bad_arguments():
         assert lib.nxs_rectify_pair_mapped_device(4096, 4096, fw, fh, maps, w, h, 4096, 4096,
                                                   None) == native.BAD_ARGUMENT
     assert lib.nxs_rectify_maps_device(None, ref, 8, 8, 8, 8, 4096, None) == native.BAD_ARGUMENT
+
+
+def test_tuning_knobs_refuse_out_of_range_and_read_back():
+    # Library-wide tuning knobs: none changes a result, each refuses a value it
+    # does not know and leaves the setting as it was.
+    lib = native.load()
+    before = lib.nxs_lean_select()
+    try:
+        assert lib.nxs_set_lean_select(17) == native.BAD_ARGUMENT
+        assert lib.nxs_lean_select() == before
+        for value in (0, 1, 16, 8):
+            assert lib.nxs_set_lean_select(value) == native.OK
+            assert lib.nxs_lean_select() == value
+    finally:
+        lib.nxs_set_lean_select(before)
+    assert lib.nxs_set_split_lanes(2) == native.BAD_ARGUMENT
+    tiles = lib.nxs_path_tiles()
+    try:
+        for mode in (0, 1, 2):
+            assert lib.nxs_set_path_tiles(mode) == native.OK
+            assert lib.nxs_path_tiles() == mode
+    finally:
+        lib.nxs_set_path_tiles(tiles)
